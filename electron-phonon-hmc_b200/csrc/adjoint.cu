@@ -1,0 +1,227 @@
+// Adjoint (reverse-mode) fermion force, sweep 2.
+//
+// Same quantity as force() + construct_all_QM1P + refine_QM1P
+// (simulation/organic_hmc.c:86-134, organic_dense_matrix.c:311-442), by a
+// different association of the same products.  With
+//   q_c(t) = Q_t e_c,  Q_t = B_{t+1}...B_{Nt-1}          (sweep 1, stored)
+//   y_c(t) = P_t^T M^-T e_c,  P_t = B_0...B_{t-1},  y_c(t+1) = B_t y_c(t)
+// the reference's G_t = Q_t M^-1 P_t is sum_c q_c(t) y_c(t)^T, and its refined
+// matrix for B_t = f_1 f_0 is
+//   D_t = sum_c (a0 q + b0 Hq)(f1 y)^T + b0 q (H f1 y)^T
+//             + (a1 f0q + b1 H f0q) y^T + b1 (f0 q)(H y)^T,
+// whose link entries D[i][n] + D[n][i] give p_dot[t,i,k] = -kappa_k flavors (...).
+// Every vector needed (Hq, f0q, H f0q, Hy, f1y, H f1y) is a by-product of
+// propagating q or y through one slice, so a slice costs 7 stencils and an
+// O(V) link contraction per vector instead of the reference's
+// (3 + log2 Nt) slice propagations of full matrices.
+//
+// One CTA owns R vectors c and walks t = 0..Nt-1, keeping all nine working
+// vectors in shared memory; partial link sums of its R vectors are added to
+// the force with one FP64 atomic per (t, site, link).
+#include "ephmc_internal.cuh"
+
+namespace ephmc {
+
+namespace {
+
+template <typename Real>
+__device__ __forceinline__ Real stencil_at(const Real *__restrict__ v, int j, const int (&src)[6],
+                                           const Real (&f)[6], Real mu) {
+    Real acc = mu * v[j];
+#pragma unroll
+    for (int e = 0; e < 6; ++e) acc = fma(f[e], v[src[e]], acc);
+    return acc;
+}
+
+template <typename Real, typename QT, int S>
+__global__ void k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
+                          const int *__restrict__ ev_fac, const int *__restrict__ nbr,
+                          const QT *__restrict__ qstack, const double *__restrict__ Minv, int V, int nt,
+                          int R, double pref_scale, double *__restrict__ force) {
+    extern __shared__ unsigned char smem_raw[];
+    Real *base = reinterpret_cast<Real *>(smem_raw);
+    const size_t RV = (size_t)R * V;
+    Real *q = base, *hq = q + RV, *f0q = hq + RV, *hf0q = f0q + RV;
+    Real *y = hf0q + RV, *hy = y + RV, *f1y = hy + RV, *hf1y = f1y + RV, *yn = hf1y + RV;
+    Real *fac = yn + RV;  // [3V]
+
+    const int T = blockDim.x, tid = threadIdx.x;
+    const int c0 = blockIdx.x * R;
+    const int nvec = min(R, V - c0);
+    const size_t VV = (size_t)V * V;
+    const Real mu = (Real)c.mu;
+    const Real al0 = (Real)c.a_lin[0], aq0 = (Real)c.a_quad[0];
+    const Real al1 = (Real)c.a_lin[1], aq1 = (Real)c.a_quad[1];
+
+    int src[S][6], nb[S][3];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int j = tid + s * T;
+#pragma unroll
+        for (int e = 0; e < 6; ++e) src[s][e] = (j < V) ? ev_src[e * V + j] : 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) nb[s][k] = (j < V) ? nbr[k * V + j] : 0;
+    }
+
+    // y(0): row c of M^-1 (math) = column c of the inverse's array
+    for (int f = tid; f < nvec * V; f += T) {
+        const int r = f % nvec, j = f / nvec;
+        y[(size_t)r * V + j] = (Real)Minv[(size_t)j * V + c0 + r];
+    }
+
+    for (int t = 0; t < nt; ++t) {
+        __syncthreads();
+        const double *xs = x + (size_t)t * 3 * V;
+        for (int e = tid; e < 3 * V; e += T) {
+            const int k = e % 3;
+            fac[e] = (Real)fma(-c.kappa[k], xs[e], c.t[k]);
+        }
+        if (t == nt - 1) {
+            for (int f = tid; f < nvec * V; f += T) {
+                const int r = f / V, j = f % V;
+                q[f] = (j == c0 + r) ? (Real)1 : (Real)0;
+            }
+        } else {
+            const QT *qs = qstack + (size_t)t * VV + (size_t)c0 * V;
+            for (int f = tid; f < nvec * V; f += T) q[f] = (Real)qs[f];
+        }
+        __syncthreads();
+        Real fl[S][6];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int j = tid + s * T;
+#pragma unroll
+            for (int e = 0; e < 6; ++e) fl[s][e] = (j < V) ? fac[ev_fac[e * V + j]] : (Real)0;
+        }
+        // A: hq = H q, hy = H y
+        for (int r = 0; r < nvec; ++r) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int j = tid + s * T;
+                if (j < V) {
+                    hq[r * V + j] = stencil_at(q + r * V, j, src[s], fl[s], mu);
+                    hy[r * V + j] = stencil_at(y + r * V, j, src[s], fl[s], mu);
+                }
+            }
+        }
+        __syncthreads();
+        // B: f0q = q + a0 hq + b0 H hq ; f1y = y + a1 hy + b1 H hy
+        for (int r = 0; r < nvec; ++r) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int j = tid + s * T;
+                if (j < V) {
+                    const Real zq = stencil_at(hq + r * V, j, src[s], fl[s], mu);
+                    f0q[r * V + j] = q[r * V + j] + fma(al0, hq[r * V + j], aq0 * zq);
+                    const Real zy = stencil_at(hy + r * V, j, src[s], fl[s], mu);
+                    f1y[r * V + j] = y[r * V + j] + fma(al1, hy[r * V + j], aq1 * zy);
+                }
+            }
+        }
+        __syncthreads();
+        // C: hf0q = H f0q, hf1y = H f1y
+        for (int r = 0; r < nvec; ++r) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int j = tid + s * T;
+                if (j < V) {
+                    hf0q[r * V + j] = stencil_at(f0q + r * V, j, src[s], fl[s], mu);
+                    hf1y[r * V + j] = stencil_at(f1y + r * V, j, src[s], fl[s], mu);
+                }
+            }
+        }
+        __syncthreads();
+        // D: yn = f0 f1 y ; contraction of the link entries
+        Real acc[S][3];
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc[s][k] = (Real)0;
+        for (int r = 0; r < nvec; ++r) {
+            const Real *Q = q + r * V, *HQ = hq + r * V, *F0Q = f0q + r * V, *HF0Q = hf0q + r * V;
+            const Real *Y = y + r * V, *HY = hy + r * V, *F1Y = f1y + r * V, *HF1Y = hf1y + r * V;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int i = tid + s * T;
+                if (i < V) {
+                    const Real z = stencil_at(HF1Y, i, src[s], fl[s], mu);
+                    yn[r * V + i] = F1Y[i] + fma(al0, HF1Y[i], aq0 * z);
+                    const Real L1i = fma(al0, Q[i], aq0 * HQ[i]);
+                    const Real L3i = fma(al1, F0Q[i], aq1 * HF0Q[i]);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int n = nb[s][k];
+                        const Real L1n = fma(al0, Q[n], aq0 * HQ[n]);
+                        const Real L3n = fma(al1, F0Q[n], aq1 * HF0Q[n]);
+                        Real d = L1i * F1Y[n];
+                        d = fma(L1n, F1Y[i], d);
+                        d = fma(aq0, fma(Q[i], HF1Y[n], Q[n] * HF1Y[i]), d);
+                        d = fma(L3i, Y[n], d);
+                        d = fma(L3n, Y[i], d);
+                        d = fma(aq1, fma(F0Q[i], HY[n], F0Q[n] * HY[i]), d);
+                        acc[s][k] += d;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const int i = tid + s * T;
+            if (i < V) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    atomicAdd(force + ((size_t)t * V + i) * 3 + k, -c.kappa[k] * pref_scale * (double)acc[s][k]);
+            }
+        }
+        __syncthreads();
+        Real *tmp = y;
+        y = yn;
+        yn = tmp;
+    }
+}
+
+}  // namespace
+
+template <typename Real, typename QT>
+int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat, const QT *qstack,
+                         const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
+                         double *force, cudaStream_t st) {
+    const int V = lat.V;
+    int S = 16;
+    for (int o : {1, 2, 4, 8, 16})
+        if ((V + o - 1) / o <= 256) { S = o; break; }
+    const int T = (((V + S - 1) / S) + 31) / 32 * 32;
+    const size_t per_vec = 9 * (size_t)V * sizeof(Real);
+    const size_t fac_b = 3 * (size_t)V * sizeof(Real);
+    const size_t budget = 200 * 1024;
+    int R = (int)((budget - fac_b) / per_vec);
+    if (R < 1) return EPHMC_ERR_UNSUPPORTED;
+    if (R > 4) R = 4;
+    const size_t smem = per_vec * R + fac_b;
+    double pref = (double)flavors;
+    if (single_particle) pref *= exp(-logdet);
+    EPHMC_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * (size_t)nt * V * 3, st));
+    void (*kern)(const double *, Couplings, const int *, const int *, const int *, const QT *, const double *,
+                 int, int, int, double, double *) = nullptr;
+    switch (S) {
+        case 1: kern = k_adjoint<Real, QT, 1>; break;
+        case 2: kern = k_adjoint<Real, QT, 2>; break;
+        case 4: kern = k_adjoint<Real, QT, 4>; break;
+        case 8: kern = k_adjoint<Real, QT, 8>; break;
+        default: kern = k_adjoint<Real, QT, 16>; break;
+    }
+    EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(V + R - 1) / R, T, smem, st>>>(x, c, lat.ev_src, lat.ev_fac, lat.nbr, qstack, Minv, V, nt, R, pref,
+                                           force); ephmc::count_launch(1);
+    EPHMC_CUDA(cudaGetLastError());
+    return EPHMC_OK;
+}
+
+template int launch_adjoint_sweep<double, double>(const double *, const Couplings &, const LatticeDev &,
+                                                  const double *, const double *, int, unsigned, int, double,
+                                                  double *, cudaStream_t);
+template int launch_adjoint_sweep<float, float>(const double *, const Couplings &, const LatticeDev &,
+                                                const float *, const double *, int, unsigned, int, double,
+                                                double *, cudaStream_t);
+
+}  // namespace ephmc

@@ -1,0 +1,600 @@
+// Device context and the native C ABI (ephmc_*): lattice tables, persistent
+// buffers and the three force+logdet algorithms.
+#include "ephmc_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+namespace ephmc {
+
+// ---------------------------------------------------------------- status
+namespace {
+thread_local int g_status = EPHMC_OK;
+thread_local unsigned g_warn = 0;
+thread_local char g_msg[512] = {0};
+}  // namespace
+
+int last_status() { return g_status; }
+unsigned last_warnings() { return g_warn; }
+const char *last_message() { return g_msg; }
+
+void set_status(int status, const char *msg) {
+    g_status = status;
+    if (msg) {
+        std::snprintf(g_msg, sizeof(g_msg), "%s", msg);
+    } else if (status == EPHMC_OK) {
+        g_msg[0] = 0;
+    }
+}
+void add_warning(unsigned bits) { g_warn |= bits; }
+void clear_status() {
+    g_status = EPHMC_OK;
+    g_warn = 0;
+    g_msg[0] = 0;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    set_status(EPHMC_ERR_CUDA, buf);
+    return EPHMC_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------- model constants
+// a = 0.5 c_p / P, a_lin = 2 Re a, a_quad = |a|^2  (simulation/organic_dense_matrix.c:169,189,192;
+// coefficients simulation/taylor-coeff_pairs.h:35-42, order {0,1} from set_taylor_pair_order :133-159)
+void pair_coefficients(double a_lin[kPairs], double a_quad[kPairs], int cplx[kPairs]) {
+    static const std::complex<double> coeff[kPairs] = {{1.8294933739891903, 0.9404019519941707},
+                                                      {0.1705066260108097, 1.5785318126884535}};
+    static const int order[kPairs] = {0, 1};
+    for (int p = 0; p < kPairs; ++p) {
+        const std::complex<double> a = 0.5 * coeff[order[p]] / (double)kPairs;
+        a_lin[p] = 2 * a.real();
+        a_quad[p] = std::pow(std::hypot(a.real(), a.imag()), 2);
+        cplx[p] = a.imag() != 0;
+    }
+}
+
+// Periodic L1 x L2 triangular lattice in the layout of construct_triangular
+// (simulation/organic_lattice.c:10-46): 6 neighbour sites per site, then 6 link indices.
+void triangular_lattice(unsigned l1, unsigned l2, unsigned *nnt) {
+    const unsigned V = l1 * l2;
+    for (unsigned i = 0; i < V; ++i) {
+        const unsigned a = i % l1, b = i / l1;
+        const unsigned right = b * l1 + (a + 1) % l1, left = b * l1 + (a + l1 - 1) % l1;
+        const unsigned up = ((b + 1) % l2) * l1, down = ((b + l2 - 1) % l2) * l1;
+        unsigned *s = nnt + 6 * i;
+        s[0] = right;
+        s[1] = left;
+        s[2] = up + a;
+        s[3] = down + a;
+        s[4] = up + (a + l1 - 1) % l1;
+        s[5] = down + (a + 1) % l1;
+        unsigned *l = nnt + 6 * (V + i);
+        l[0] = 3 * i;
+        l[1] = 3 * s[1];
+        l[2] = 3 * i + 1;
+        l[3] = 3 * s[3] + 1;
+        l[4] = 3 * i + 2;
+        l[5] = 3 * s[5] + 2;
+    }
+}
+
+// The reference's scatter loop (apply_mu_K_to_v, simulation/organic_dense_matrix.c:100-119)
+// visits (i, k) in order and adds fac_ik v[n] into w[i] ("here") then fac_ik v[i] into
+// w[n] ("there").  For the gather form, list for every site the six terms it
+// receives, sorted by (i, k, here-before-there).  Only the forward entries
+// nnt[6i+2k] are read, as in the reference.
+int build_event_tables(const unsigned *nnt, int V, std::vector<int> &ev_src, std::vector<int> &ev_fac,
+                       std::vector<int> &nbr) {
+    struct Ev {
+        long key;
+        int src, fac;
+    };
+    std::vector<std::vector<Ev>> per(V);
+    nbr.assign(3 * (size_t)V, 0);
+    for (int i = 0; i < V; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            const unsigned n = nnt[6 * (size_t)i + 2 * k];
+            if (n >= (unsigned)V) return EPHMC_ERR_LATTICE;
+            nbr[(size_t)k * V + i] = (int)n;
+            const long base = ((long)i * 3 + k) * 2;
+            per[i].push_back({base, (int)n, 3 * i + k});
+            per[n].push_back({base + 1, i, 3 * i + k});
+        }
+    }
+    ev_src.assign(6 * (size_t)V, 0);
+    ev_fac.assign(6 * (size_t)V, 0);
+    for (int j = 0; j < V; ++j) {
+        if (per[j].size() != 6) return EPHMC_ERR_LATTICE;
+        std::sort(per[j].begin(), per[j].end(), [](const Ev &a, const Ev &b) { return a.key < b.key; });
+        for (int e = 0; e < 6; ++e) {
+            ev_src[(size_t)e * V + j] = per[j][e].src;
+            ev_fac[(size_t)e * V + j] = per[j][e].fac;
+        }
+    }
+    return EPHMC_OK;
+}
+
+}  // namespace ephmc
+
+using namespace ephmc;
+
+namespace {
+
+bool is_device_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int ret(int status, const char *msg = nullptr) {
+    if (status != EPHMC_OK) set_status(status, msg);
+    return status;
+}
+
+unsigned ceil_half(unsigned n) { return n / 2 + n % 2; }  // simulation/organic_aux.c:11-13
+unsigned ceil_log2(unsigned n) {                          // simulation/organic_aux.c:15-19
+    unsigned l = 0;
+    while (n > 1) {
+        n = ceil_half(n);
+        ++l;
+    }
+    return l;
+}
+
+void set_couplings(ephmc_ctx *c, const double t[3], const double kappa[3], double mu) {
+    for (int k = 0; k < 3; ++k) {
+        c->c.t[k] = t[k];
+        c->c.kappa[k] = kappa[k];
+    }
+    c->c.mu = mu;
+    pair_coefficients(c->c.a_lin, c->c.a_quad, c->c.cplx);
+}
+
+int ensure_jobs(ephmc_ctx *c, int n) {
+    if (n <= c->jobs_cap) return EPHMC_OK;
+    return ret(EPHMC_ERR_ARG, "job table too small");
+}
+
+int upload_jobs(ephmc_ctx *c, const std::vector<SliceJob> &jobs, SliceJob *dst) {
+    if (jobs.empty()) return EPHMC_OK;
+    EPHMC_CUDA(cudaMemcpyAsync(dst, jobs.data(), sizeof(SliceJob) * jobs.size(), cudaMemcpyHostToDevice, c->stream));
+    return EPHMC_OK;
+}
+
+SliceJob job(const void *src, void *dst, int s_first, int s_count, int s_dir, int pb, int pe, int ps) {
+    SliceJob j{};
+    j.src = src;
+    j.dst = dst;
+    j.stack = nullptr;
+    j.stack_off = 0;
+    j.s_first = s_first;
+    j.s_count = s_count;
+    j.s_dir = s_dir;
+    j.p_begin = pb;
+    j.p_end = pe;
+    j.p_step = ps;
+    j.add_identity = 0;
+    return j;
+}
+
+// stage a caller pointer: device pointers are used in place, host ones copied
+int stage_in(ephmc_ctx *c, const double *user, double *devbuf, size_t n, const double **out) {
+    if (is_device_ptr(user)) {
+        *out = user;
+        return EPHMC_OK;
+    }
+    EPHMC_CUDA(cudaMemcpyAsync(devbuf, user, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    *out = devbuf;
+    return EPHMC_OK;
+}
+
+int stage_out(ephmc_ctx *c, double *user, const double *devbuf, size_t n) {
+    if (!user || user == devbuf) return EPHMC_OK;
+    if (is_device_ptr(user)) {
+        EPHMC_CUDA(cudaMemcpyAsync(user, devbuf, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        EPHMC_CUDA(cudaMemcpyAsync(user, devbuf, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    return EPHMC_OK;
+}
+
+// M_hat (or, with a stack, sweep 1 of the adjoint) into c->M
+int build_M_hat(ephmc_ctx *c, const double *x, void *stack, bool stack_float) {
+    SliceJob j = job(nullptr, c->M, (int)c->nt - 1, (int)c->nt, -1, 0, kPairs, 1);
+    j.add_identity = !(c->flags.zero_filling || c->flags.single_particle);
+    j.stack = stack;
+    j.stack_off = -1;
+    std::vector<SliceJob> v{j};
+    int rc = upload_jobs(c, v, c->jobs);
+    if (rc) return rc;
+    if (stack && stack_float)
+        return launch_slices<double, double, float>(Axis::Rows, x, c->c, c->lat, c->jobs, 1, c->stream);
+    return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs, 1, c->stream);
+}
+
+int factor(ephmc_ctx *c, double *logdet, int *ipiv_host) {
+    int sign = 1;
+    double ld = 0;
+    int rc = lu_logdet_inverse(c->M, c->lu, &ld, &sign, ipiv_host, c->stream);
+    c->last_logdet = ld;
+    c->last_sign = sign;
+    if (logdet) *logdet = ld;
+    if (rc == EPHMC_OK && sign < 0 && (c->flavors % 2)) add_warning(EPHMC_WARN_NEGATIVE_DET);
+    c->have_inverse = (rc == EPHMC_OK);
+    return rc;
+}
+
+// construct_all_QM1P (simulation/organic_dense_matrix.c:311-381) as batched launches:
+// per halving pass, every spawned copy (P side, on columns) in one launch, then
+// every Q-side extension (on rows) in one launch.
+int all_G(ephmc_ctx *c, const double *x) {
+    const unsigned nt = c->nt;
+    const size_t VV = (size_t)c->V * c->V;
+    int rc;
+    if (!c->flags.single_particle) rc = launch_copy(c->G, c->M, VV, c->stream);
+    else rc = launch_identity(c->G, (int)c->V, c->stream);
+    if (rc) return rc;
+    std::vector<unsigned> from_q(nt, 0), from_p(nt, 0);
+    unsigned left = nt - 1;
+    const unsigned passes = ceil_log2(nt);
+    for (unsigned r = 0; r < passes; ++r) {
+        const unsigned chunk = ceil_half(left);
+        std::vector<SliceJob> spawn, ext;
+        for (int i = (int)nt - 1; i >= 0; --i) {
+            if (!(i == 0 || from_q[i] || from_p[i])) continue;
+            const unsigned j = (unsigned)i + chunk;
+            double *Gi = c->G + (size_t)i * VV;
+            if (j < nt && from_q[j] == 0 && from_p[j] == 0) {
+                spawn.push_back(job(Gi, c->G + (size_t)j * VV, (int)from_p[i], (int)chunk, +1, 0, kPairs, 1));
+                from_q[j] = from_q[i];
+                from_p[j] = from_p[i] + chunk;
+            }
+            ext.push_back(job(Gi, Gi, (int)(nt - 1 - from_q[i]), (int)chunk, -1, 0, kPairs, 1));
+            from_q[i] += chunk;
+        }
+        left -= chunk;
+        if ((rc = ensure_jobs(c, (int)(spawn.size() + ext.size())))) return rc;
+        if ((rc = upload_jobs(c, spawn, c->jobs))) return rc;
+        if ((rc = upload_jobs(c, ext, c->jobs + spawn.size()))) return rc;
+        if ((rc = launch_slices<double, double, double>(Axis::Cols, x, c->c, c->lat, c->jobs, (int)spawn.size(),
+                                                        c->stream)))
+            return rc;
+        if ((rc = launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs + spawn.size(),
+                                                        (int)ext.size(), c->stream)))
+            return rc;
+    }
+    if (left != 0) return ret(EPHMC_ERR_UNSUPPORTED, "log-depth sharing left slices unaccounted");
+    for (unsigned i = 0; i < nt; ++i)
+        if (from_q[i] + from_p[i] != nt - 1) return ret(EPHMC_ERR_UNSUPPORTED, "G_t bookkeeping mismatch");
+    return EPHMC_OK;
+}
+
+// refine_QM1P + force contraction for every slice, in batches of refine_batch slices
+int refine_all(ephmc_ctx *c, const double *x, double logdet) {
+    const unsigned nt = c->nt;
+    const size_t VV = (size_t)c->V * c->V;
+    const int nb = c->refine_batch;
+    int rc;
+    for (unsigned t0 = 0; t0 < nt; t0 += nb) {
+        const int cnt = (int)std::min<unsigned>(nb, nt - t0);
+        std::vector<SliceJob> cols, rows;
+        for (int b = 0; b < cnt; ++b) {
+            const double *Gt = c->G + (size_t)(t0 + b) * VV;
+            // pair 0: X_0 = G F_>0 -> pair 1 on columns (transpose, apply_exp revert, :410-413)
+            cols.push_back(job(Gt, c->A + (size_t)b * VV, (int)(t0 + b), 1, 1, 1, 2, 1));
+            // pair 1: X_1 = F_<1 G -> pair 0 on rows (apply_exp forward, :408)
+            rows.push_back(job(Gt, c->B + (size_t)b * VV, (int)(t0 + b), 1, 1, 0, 1, 1));
+        }
+        if ((rc = upload_jobs(c, cols, c->jobs))) return rc;
+        if ((rc = upload_jobs(c, rows, c->jobs + cnt))) return rc;
+        if ((rc = launch_slices<double, double, double>(Axis::Cols, x, c->c, c->lat, c->jobs, cnt, c->stream)))
+            return rc;
+        if ((rc = launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs + cnt, cnt,
+                                                        c->stream)))
+            return rc;
+        if ((rc = launch_link_refine(x, c->c, c->lat, c->A, c->B, (int)t0, cnt, c->flavors, c->flags.schur_form_inv,
+                                     c->flags.single_particle, logdet, c->force, c->stream)))
+            return rc;
+    }
+    return EPHMC_OK;
+}
+
+}  // namespace
+
+
+extern "C" {
+
+int ephmc_last_status(void) { return ephmc::last_status(); }
+unsigned ephmc_last_warnings(void) { return ephmc::last_warnings(); }
+const char *ephmc_last_error_message(void) { return ephmc::last_message(); }
+
+const char *ephmc_status_string(int s) {
+    switch (s) {
+        case EPHMC_OK: return "ok";
+        case EPHMC_ERR_CUDA: return "CUDA runtime error";
+        case EPHMC_ERR_ARG: return "invalid argument";
+        case EPHMC_ERR_LATTICE: return "neighbour table is not a periodic triangular lattice";
+        case EPHMC_ERR_SINGULAR: return "singular fermion matrix (zero pivot)";
+        case EPHMC_ERR_NONFINITE: return "non-finite log det or force";
+        case EPHMC_ERR_NOMEM: return "device allocation failed";
+        case EPHMC_ERR_UNSUPPORTED: return "unsupported on the GPU path";
+        case EPHMC_ERR_TIMEOUT: return "bounded device wait gave up";
+        case EPHMC_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char *ephmc_version(void) { return "ephmc 0.1 (sm_100a)"; }
+
+void *ephmc_alloc(size_t bytes) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_status(EPHMC_ERR_NOMEM, "ephmc_alloc");
+        return nullptr;
+    }
+    return p;
+}
+void ephmc_free(void *p) {
+    if (p) cudaFree(p);
+}
+int ephmc_memcpy_h2d(void *dst, const void *src, size_t bytes) {
+    EPHMC_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    return EPHMC_OK;
+}
+int ephmc_memcpy_d2h(void *dst, const void *src, size_t bytes) {
+    EPHMC_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    return EPHMC_OK;
+}
+int ephmc_device_synchronize(void) {
+    EPHMC_CUDA(cudaDeviceSynchronize());
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_destroy(ephmc_ctx *c) {
+    if (!c) return EPHMC_OK;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(c->device);
+    void *bufs[] = {c->x, c->force, c->M, c->G, c->A, c->B, c->qstack, c->jobs, c->lat.ev_src, c->lat.ev_fac,
+                    c->lat.nbr, c->scratch};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    lu_free(c->lu);
+    for (auto &e : c->ev)
+        if (e) cudaEventDestroy(e);
+    cudaSetDevice(cur);
+    delete c;
+    return EPHMC_OK;
+}
+
+static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsigned *nnt_in, unsigned V,
+                           unsigned nt, const double t[3], const double kappa[3], double mu, double omega,
+                           unsigned flavors, const ephmc_flags *flags, int device) {
+    clear_status();
+    if (!out || V == 0 || nt == 0 || !t || !kappa) return ret(EPHMC_ERR_ARG, "ephmc_ctx_create arguments");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return ret(EPHMC_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0) EPHMC_CUDA(cudaGetDevice(&device));
+    EPHMC_CUDA(cudaSetDevice(device));
+    ephmc_ctx *c = new (std::nothrow) ephmc_ctx();
+    if (!c) return ret(EPHMC_ERR_NOMEM, "host allocation");
+    c->device = device;
+    c->l1 = l1;
+    c->l2 = l2;
+    c->V = V;
+    c->nt = nt;
+    c->flavors = flavors;
+    c->omega = omega;
+    if (flags) c->flags = *flags;
+    set_couplings(c, t, kappa, mu);
+    c->nnt.resize(12 * (size_t)V);
+    if (nnt_in) std::memcpy(c->nnt.data(), nnt_in, sizeof(unsigned) * 12 * V);
+    else triangular_lattice(l1, l2, c->nnt.data());
+    std::vector<int> es, ef, nb;
+    int rc = build_event_tables(c->nnt.data(), (int)V, es, ef, nb);
+    if (rc) {
+        delete c;
+        return ret(rc, "neighbour table: every site must receive exactly three forward links");
+    }
+    c->lat.V = (int)V;
+    c->lat.l1 = (int)l1;
+    c->lat.l2 = (int)l2;
+    const size_t VV = (size_t)V * V, dim = (size_t)nt * V * 3;
+    c->refine_batch = (int)std::min<unsigned>(nt, 16);
+    c->jobs_cap = (int)std::max<unsigned>(2 * nt, 2 * (unsigned)c->refine_batch) + 8;
+    c->scratch_n = fa_scratch_doubles(3 * (int)V, (int)nt) + 16;
+    auto fail = [&](cudaError_t e, const char *what) {
+        cuda_fail(e, what);
+        cudaGetLastError();
+        ephmc_ctx_destroy(c);
+        return (e == cudaErrorMemoryAllocation) ? ret(EPHMC_ERR_NOMEM, what) : EPHMC_ERR_CUDA;
+    };
+#define ALLOC(ptr, bytes)                                   \
+    do {                                                    \
+        cudaError_t _e = cudaMalloc((void **)&(ptr), bytes); \
+        if (_e != cudaSuccess) return fail(_e, #ptr);       \
+    } while (0)
+    ALLOC(c->lat.ev_src, sizeof(int) * 6 * V);
+    ALLOC(c->lat.ev_fac, sizeof(int) * 6 * V);
+    ALLOC(c->lat.nbr, sizeof(int) * 3 * V);
+    ALLOC(c->x, sizeof(double) * dim);
+    ALLOC(c->force, sizeof(double) * dim);
+    ALLOC(c->M, sizeof(double) * VV);
+    ALLOC(c->G, sizeof(double) * VV * nt);
+    ALLOC(c->A, sizeof(double) * VV * c->refine_batch);
+    ALLOC(c->B, sizeof(double) * VV * c->refine_batch);
+    c->qstack_bytes = sizeof(double) * VV * nt;
+    ALLOC(c->qstack, c->qstack_bytes);
+    ALLOC(c->jobs, sizeof(SliceJob) * c->jobs_cap);
+    ALLOC(c->scratch, sizeof(double) * c->scratch_n);
+#undef ALLOC
+    if (lu_alloc(c->lu, (int)V) != EPHMC_OK) {
+        ephmc_ctx_destroy(c);
+        return ret(EPHMC_ERR_NOMEM, "LU workspace");
+    }
+    cudaMemcpy(c->lat.ev_src, es.data(), sizeof(int) * 6 * V, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->lat.ev_fac, ef.data(), sizeof(int) * 6 * V, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->lat.nbr, nb.data(), sizeof(int) * 3 * V, cudaMemcpyHostToDevice);
+    for (auto &e : c->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            ephmc_ctx_destroy(c);
+            return ret(EPHMC_ERR_CUDA, "cudaEventCreate");
+        }
+    if (cudaGetLastError() != cudaSuccess) {
+        ephmc_ctx_destroy(c);
+        return ret(EPHMC_ERR_CUDA, "context upload");
+    }
+    *out = c;
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_create(ephmc_ctx **out, unsigned l1, unsigned l2, unsigned nt, const double t[3],
+                     const double kappa[3], double mu, double omega, unsigned flavors, const ephmc_flags *flags,
+                     int device) {
+    if (l1 == 0 || l2 == 0) return ret(EPHMC_ERR_ARG, "lattice extent");
+    return ctx_create_impl(out, l1, l2, nullptr, l1 * l2, nt, t, kappa, mu, omega, flavors, flags, device);
+}
+
+int ephmc_ctx_create_nnt(ephmc_ctx **out, const unsigned *nnt, unsigned ns, unsigned nt, const double t[3],
+                         const double kappa[3], double mu, double omega, unsigned flavors, const ephmc_flags *flags,
+                         int device) {
+    if (!nnt) return ret(EPHMC_ERR_ARG, "nnt");
+    return ctx_create_impl(out, 0, 0, nnt, ns, nt, t, kappa, mu, omega, flavors, flags, device);
+}
+
+int ephmc_ctx_set_params(ephmc_ctx *c, const double t[3], const double kappa[3], double mu, double omega,
+                         unsigned flavors) {
+    if (!c || !t || !kappa) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_params");
+    set_couplings(c, t, kappa, mu);
+    c->omega = omega;
+    c->flavors = flavors;
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_set_flags(ephmc_ctx *c, const ephmc_flags *flags) {
+    if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_flags");
+    c->flags = flags ? *flags : ephmc_flags{};
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_lattice(const ephmc_ctx *c, unsigned *nnt_out) {
+    if (!c || !nnt_out) return ret(EPHMC_ERR_ARG, "ephmc_ctx_lattice");
+    std::memcpy(nnt_out, c->nnt.data(), sizeof(unsigned) * c->nnt.size());
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_set_stream(ephmc_ctx *c, void *stream) {
+    if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_stream");
+    c->stream = static_cast<cudaStream_t>(stream);
+    return EPHMC_OK;
+}
+
+int ephmc_construct_M_hat(ephmc_ctx *c, const double *x, double *M_hat_out) {
+    clear_status();
+    if (!c || !x) return ret(EPHMC_ERR_ARG, "ephmc_construct_M_hat");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t dim = (size_t)c->nt * c->V * 3;
+    const double *xd = nullptr;
+    int rc;
+    if ((rc = stage_in(c, x, c->x, dim, &xd))) return ret(rc);
+    if ((rc = build_M_hat(c, xd, nullptr, false))) return ret(rc);
+    c->have_inverse = false;
+    if ((rc = stage_out(c, M_hat_out, c->M, (size_t)c->V * c->V))) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    return EPHMC_OK;
+}
+
+int ephmc_logdet_inverse(ephmc_ctx *c, double *M, int *ipiv, double *logdet, int *sign) {
+    clear_status();
+    if (!c || !M) return ret(EPHMC_ERR_ARG, "ephmc_logdet_inverse");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t VV = (size_t)c->V * c->V;
+    const double *Md = nullptr;
+    int rc;
+    if ((rc = stage_in(c, M, c->M, VV, &Md))) return ret(rc);
+    if (Md != c->M) EPHMC_CUDA(cudaMemcpyAsync(c->M, Md, sizeof(double) * VV, cudaMemcpyDeviceToDevice, c->stream));
+    rc = factor(c, logdet, ipiv);
+    if (sign) *sign = c->last_sign;
+    if (rc) return ret(rc, rc == EPHMC_ERR_SINGULAR ? "zero pivot" : nullptr);
+    if ((rc = stage_out(c, M, c->M, VV))) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_get_inverse(ephmc_ctx *c, double *out) {
+    if (!c || !out) return ret(EPHMC_ERR_ARG, "ephmc_ctx_get_inverse");
+    if (!c->have_inverse) return ret(EPHMC_ERR_ARG, "no inverse computed yet");
+    int rc = stage_out(c, out, c->M, (size_t)c->V * c->V);
+    if (rc) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_last_timings(const ephmc_ctx *c, float *a, float *b, float *d) {
+    if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_last_timings");
+    if (a) *a = c->t_mhat;
+    if (b) *b = c->t_lu;
+    if (d) *d = c->t_force;
+    return EPHMC_OK;
+}
+
+int ephmc_eval(ephmc_ctx *c, const double *x, double *p_dot, double *logdet, int mode) {
+    clear_status();
+    if (!c || !x) return ret(EPHMC_ERR_ARG, "ephmc_eval");
+    if (mode < EPHMC_FORCE_REFERENCE || mode > EPHMC_FORCE_MIXED) return ret(EPHMC_ERR_ARG, "force mode");
+    const ephmc_flags &f = c->flags;
+    if (f.schur_form_inv || f.constant_force || f.single_particle || f.zero_filling)
+        return ret(EPHMC_ERR_UNSUPPORTED, "flag not implemented on the GPU path");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t dim = (size_t)c->nt * c->V * 3;
+    const double *xd = nullptr;
+    int rc;
+    if ((rc = stage_in(c, x, c->x, dim, &xd))) return ret(rc);
+    EPHMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    const bool adj = mode != EPHMC_FORCE_REFERENCE;
+    const bool mixed = mode == EPHMC_FORCE_MIXED;
+    if ((rc = build_M_hat(c, xd, adj ? c->qstack : nullptr, mixed))) return ret(rc);
+    EPHMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    double ld = 0;
+    rc = factor(c, &ld, nullptr);
+    if (rc) return ret(rc, rc == EPHMC_ERR_SINGULAR ? "zero pivot" : nullptr);
+    EPHMC_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    if (!adj) {
+        if ((rc = all_G(c, xd))) return ret(rc);
+        if ((rc = refine_all(c, xd, ld))) return ret(rc);
+    } else if (!mixed) {
+        rc = launch_adjoint_sweep<double, double>(xd, c->c, c->lat, static_cast<const double *>(c->qstack), c->M,
+                                                  (int)c->nt, c->flavors, f.single_particle, ld, c->force,
+                                                  c->stream);
+        if (rc) return ret(rc);
+    } else {
+        rc = launch_adjoint_sweep<float, float>(xd, c->c, c->lat, static_cast<const float *>(c->qstack), c->M,
+                                                (int)c->nt, c->flavors, f.single_particle, ld, c->force, c->stream);
+        if (rc) return ret(rc);
+    }
+    EPHMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    if ((rc = stage_out(c, p_dot, c->force, dim))) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    cudaEventElapsedTime(&c->t_mhat, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&c->t_lu, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&c->t_force, c->ev[2], c->ev[3]);
+    if (logdet) *logdet = ld;
+    if (!std::isfinite(ld)) return ret(EPHMC_ERR_NONFINITE, "log det not finite");
+    return EPHMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+// Internal declarations shared by the CUDA translation units of libephmc_cuda.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ephmc.h"
+
+namespace ephmc {
+
+constexpr int kPairs = 2;  // Taylor-4 as two quadratic pairs (simulation/taylor-coeff_pairs.h:35-42)
+
+// ---------------------------------------------------------------- status plumbing
+void set_status(int status, const char *msg = nullptr);
+int last_status();
+unsigned last_warnings();
+const char *last_message();
+void add_warning(unsigned bits);
+void clear_status();
+int cuda_fail(cudaError_t e, const char *what);
+void count_launch(unsigned n);  // kernel launches issued by this library (diag.cu)
+
+#define EPHMC_CUDA(call)                                              \
+    do {                                                              \
+        cudaError_t _e = (call);                                      \
+        if (_e != cudaSuccess) return ::ephmc::cuda_fail(_e, #call);  \
+    } while (0)
+
+// ---------------------------------------------------------------- model constants
+// Lattice-unit couplings and the Taylor pair coefficients, passed by value to kernels.
+struct Couplings {
+    double t[3];
+    double kappa[3];
+    double mu;
+    double a_lin[kPairs];   // 2 Re a_p,  a_p = c_p / (2P)
+    double a_quad[kPairs];  // |a_p|^2
+    int cplx[kPairs];       // Im a_p != 0
+};
+
+void pair_coefficients(double a_lin[kPairs], double a_quad[kPairs], int cplx[kPairs]);
+
+// Device-resident lattice tables derived from the neighbour table nnt.
+//   ev_src[e*V + j], ev_fac[e*V + j], e = 0..5: the six hopping terms that the
+//   reference's scatter loop (simulation/organic_dense_matrix.c:103-119) adds
+//   into w[j], in the order it adds them: operand site and coefficient index
+//   (3*site + link) of the slice's hopping table.
+//   nbr[k*V + i]: forward neighbour of site i along link k (nnt[6i+2k]).
+struct LatticeDev {
+    int V = 0;
+    int l1 = 0, l2 = 0;
+    int *ev_src = nullptr;
+    int *ev_fac = nullptr;
+    int *nbr = nullptr;
+};
+
+// Host helper: build the event tables; returns EPHMC_OK or EPHMC_ERR_LATTICE.
+int build_event_tables(const unsigned *nnt, int V, std::vector<int> &ev_src,
+                       std::vector<int> &ev_fac, std::vector<int> &nbr);
+void triangular_lattice(unsigned l1, unsigned l2, unsigned *nnt);
+
+// ---------------------------------------------------------------- slice propagation
+// One job = one V x V matrix whose vectors (rows, or columns) get a sequence
+// of slice propagators, optionally spilling the state after each slice.
+struct SliceJob {
+    const void *src;       // input matrix; nullptr = start from the identity
+    void *dst;             // output matrix (may equal src)
+    void *stack;           // optional: state after slice s goes to stack[(s + stack_off) * V*V]
+    int stack_off;
+    int s_first, s_count, s_dir;  // slices s_first, s_first + s_dir, ...
+    int p_begin, p_end, p_step;   // pairs p_begin, p_begin+p_step, ... != p_end
+    int add_identity;             // dst[i][i] += 1 after the last slice
+};
+
+enum class Axis { Rows, Cols };
+
+// Launch a batch of jobs on all vectors of every job matrix.
+//   Real: arithmetic type; Store: element type of src/dst; StackT: of stack.
+template <typename Real, typename Store, typename StackT>
+int launch_slices(Axis axis, const double *x, const Couplings &c, const LatticeDev &lat,
+                  const SliceJob *jobs_dev, int njobs, cudaStream_t st);
+
+// Reference-algorithm refinement + link contraction for slices t0..t0+nb-1:
+//   A_t = pair 1 on columns of G_t, B_t = pair 0 on rows of G_t (already formed),
+//   force[t][i][k] from the link entries of
+//   D = a0 A + q0 (H A + A H) + a1 B + q1 (H B + B H)   (refine_QM1P, :383-442).
+int launch_link_refine(const double *x, const Couplings &c, const LatticeDev &lat,
+                       const double *A, const double *B, int t0, int nb, unsigned flavors,
+                       int schur_clamp, int single_particle, double logdet, double *force,
+                       cudaStream_t st);
+
+// Adjoint sweep 2 (see adjoint.cu): y chain forward from M^-1, contraction with
+// the stored q(t).
+template <typename Real, typename QT>
+int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat,
+                         const QT *qstack, const double *Minv, int nt, unsigned flavors,
+                         int single_particle, double logdet, double *force, cudaStream_t st);
+
+// ---------------------------------------------------------------- dense helpers
+int launch_copy(double *dst, const double *src, size_t n, cudaStream_t st);
+int launch_identity(double *M, int V, cudaStream_t st);
+int launch_transpose(double *M, int V, cudaStream_t st);
+int launch_fill(double *p, double v, size_t n, cudaStream_t st);
+
+// ---------------------------------------------------------------- LU
+struct LUWork {
+    int V = 0;
+    int *ipiv = nullptr;       // device, 0-based pivot rows
+    double *diag = nullptr;    // device, U_ii
+    int *info = nullptr;       // device flag
+    double *X = nullptr;       // device V*V, receives the inverse before it is copied back
+};
+int lu_alloc(LUWork &w, int V);
+void lu_free(LUWork &w);
+// In-place LU with partial pivoting of the column-major matrix A(r,c) = M[c*V+r],
+// followed by the in-place inverse; log|det| and sign into host outputs.
+int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv_host,
+                      cudaStream_t st);
+
+// ---------------------------------------------------------------- Fourier acceleration
+// scratch: device doubles, at least fa_scratch_doubles(ld, nt)
+size_t fa_scratch_doubles(int ld, int nt);
+int fa_evolve(double *x, double *p, int ld, int nt, double omega, double h, double *scratch, cudaStream_t st);
+int fa_scale_modes(double *v, int ld, int nt, double omega, int mode, double *scratch, cudaStream_t st);
+int fa_energy(const double *p, int ld, int nt, double omega, double *out_dev, double *scratch, cudaStream_t st);
+
+}  // namespace ephmc
+
+// ---------------------------------------------------------------- context
+struct ephmc_ctx {
+    int device = 0;
+    unsigned l1 = 0, l2 = 0, V = 0, nt = 0, flavors = 1;
+    double omega = 0;
+    ephmc_flags flags{};
+    ephmc::Couplings c{};
+    ephmc::LatticeDev lat{};
+    std::vector<unsigned> nnt;
+    cudaStream_t stream = nullptr;
+
+    // persistent device buffers
+    double *x = nullptr;      // nt*V*3
+    double *force = nullptr;  // nt*V*3
+    double *M = nullptr;      // V*V  (M_hat, then its inverse)
+    double *G = nullptr;      // nt*V*V (reference algorithm)
+    double *A = nullptr;      // nb*V*V refine scratch
+    double *B = nullptr;      // nb*V*V refine scratch
+    int refine_batch = 0;
+    void *qstack = nullptr;   // (nt)*V*V (adjoint), FP64 or FP32
+    size_t qstack_bytes = 0;
+    ephmc::SliceJob *jobs = nullptr;  // device job array
+    int jobs_cap = 0;
+    std::vector<ephmc::SliceJob> jobs_host;
+    ephmc::LUWork lu{};
+    double last_logdet = 0;
+    int last_sign = 1;
+    bool have_inverse = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float t_mhat = 0, t_lu = 0, t_force = 0;
+    double *scratch = nullptr;  // small device scratch (Fourier mode tables, reductions)
+    size_t scratch_n = 0;
+};

@@ -1,0 +1,188 @@
+/*
+ * ephmc -- B200-native (sm_100a) CUDA implementation of the Hybrid Monte Carlo
+ * hot path of j-ostmeyer/electron-phonon-hmc, exposed as a C ABI.
+ *
+ * Two surfaces, both exported by libephmc_cuda.so:
+ *
+ *  1. The drop-in surface: the reference's own functions with identical names
+ *     and prototypes (declared in ephmc_organic.h), so the reference's C host
+ *     code links against this library in place of organic_dense_matrix.o,
+ *     organic_hmc.o and organic_bosons.o.
+ *
+ *  2. The native surface below (prefix ephmc_): a device context that keeps
+ *     the lattice, parameters and every work buffer resident on one GPU and
+ *     evaluates log det M and the fermion force in one call, in one of three
+ *     algorithms.
+ *
+ * Pointers: every double* argument of the native surface may be a device
+ * pointer (used in place) or a host pointer (staged through the context's
+ * device buffers, copies included in the call).  Sizes are plain unsigned.
+ * No call allocates device memory after ephmc_ctx_create except
+ * ephmc_ctx_create itself and the explicit ephmc_alloc.
+ *
+ * Errors: every ephmc_ function returns an ephmc_status; the most recent
+ * status of the calling thread, including calls made through the drop-in
+ * surface, is available from ephmc_last_status().
+ */
+#ifndef EPHMC_H
+#define EPHMC_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define EPHMC_API __attribute__((visibility("default")))
+#else
+#define EPHMC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum {
+    EPHMC_OK = 0,
+    EPHMC_ERR_CUDA = 1,        /* a CUDA runtime call failed (message via ephmc_last_error_message) */
+    EPHMC_ERR_ARG = 2,         /* invalid argument (size, pointer, mode) */
+    EPHMC_ERR_LATTICE = 3,     /* neighbour table is not a periodic triangular lattice */
+    EPHMC_ERR_SINGULAR = 4,    /* exact zero pivot in the LU factorisation */
+    EPHMC_ERR_NONFINITE = 5,   /* log det or force is not finite */
+    EPHMC_ERR_NOMEM = 6,       /* device allocation failed */
+    EPHMC_ERR_UNSUPPORTED = 7, /* flag combination or size not implemented on the GPU path */
+    EPHMC_ERR_TIMEOUT = 8,     /* a bounded device-side wait gave up */
+    EPHMC_ERR_NO_DEVICE = 9    /* no CUDA device / extension not usable */
+} ephmc_status;
+
+/* warning bits reported alongside EPHMC_OK (ephmc_last_warnings) */
+#define EPHMC_WARN_NEGATIVE_DET 0x1u /* "Negative determinant!" of
+                                        simulation/organic_dense_matrix.c:589 */
+
+EPHMC_API int ephmc_last_status(void);
+EPHMC_API unsigned ephmc_last_warnings(void);
+EPHMC_API const char *ephmc_status_string(int status);
+EPHMC_API const char *ephmc_last_error_message(void);
+
+/* ------------------------------------------------------------------ force algorithms */
+typedef enum {
+    /* The reference algorithm in FP64: M_hat by Nt slice propagations,
+     * dgetrf/dgetri-equivalent LU, G_t = Q_t M^-1 P_t by the log-depth
+     * sharing of construct_all_QM1P, refine_QM1P and the link contraction
+     * (simulation/organic_dense_matrix.c:251-442, organic_hmc.c:86-134).
+     * Stencil sums run in the reference's order, so M_hat is bit-identical
+     * to the reference's. */
+    EPHMC_FORCE_REFERENCE = 0,
+    /* Reverse-mode (adjoint) accumulation of d log det / dx in FP64:
+     * O(Nt) slice propagations instead of O(Nt log Nt), no G_t matrices. */
+    EPHMC_FORCE_ADJOINT_FP64 = 1,
+    /* Adjoint with FP64 M_hat, LU and log det, and FP32 propagation and
+     * contraction of the force (the mixed-precision MD force). */
+    EPHMC_FORCE_MIXED = 2
+} ephmc_force_mode;
+
+/* organic_flags (simulation/organic_flags.h:4-14), same layout */
+typedef struct ephmc_flags {
+    int schur_form_inv;
+    int zero_filling;
+    int static_disorder;
+    int single_particle;
+    int constant_force;
+    int no_fourier_acc;
+    int classical_fourier_acc;
+    unsigned cfa_steps;
+    double cfa_mass;
+} ephmc_flags;
+
+/* ------------------------------------------------------------------ context */
+typedef struct ephmc_ctx ephmc_ctx;
+
+/* Model in lattice units, as run_hmc receives it (simulation/organic_hmc.c:296):
+ * L1 x L2 periodic triangular lattice, nt slices, hoppings t[3], couplings
+ * kappa[3], chemical potential mu, phonon frequency omega, fermion flavours.
+ * flags may be NULL (all off).  device: CUDA ordinal (-1 = current). */
+EPHMC_API int ephmc_ctx_create(ephmc_ctx **out, unsigned l1, unsigned l2, unsigned nt,
+                     const double t[3], const double kappa[3], double mu,
+                     double omega, unsigned flavors, const ephmc_flags *flags,
+                     int device);
+EPHMC_API int ephmc_ctx_destroy(ephmc_ctx *ctx);
+
+/* Change the couplings of an existing context (no reallocation). */
+EPHMC_API int ephmc_ctx_set_params(ephmc_ctx *ctx, const double t[3], const double kappa[3],
+                         double mu, double omega, unsigned flavors);
+
+/* Neighbour table of the context, 12*V entries in the layout of
+ * construct_triangular (simulation/organic_lattice.c:10-46); host pointer. */
+EPHMC_API int ephmc_ctx_lattice(const ephmc_ctx *ctx, unsigned *nnt_out);
+
+/* Bind the context to a CUDA stream (cudaStream_t passed as void*); 0 = legacy default. */
+EPHMC_API int ephmc_ctx_set_stream(ephmc_ctx *ctx, void *stream);
+
+/* One force+logdet evaluation, the body of leap_frog
+ * (simulation/organic_hmc.c:177-180):
+ *   x[nt*V*3]      phonon field, layout [t][site][link]       (in)
+ *   p_dot[nt*V*3]  fermion force = flavors * d log det / dx    (out, may be NULL)
+ *   logdet         log|det M_hat|                              (out, host, may be NULL)
+ * The inverse M_hat^-1 stays in the context (ephmc_ctx_get_inverse). */
+EPHMC_API int ephmc_eval(ephmc_ctx *ctx, const double *x, double *p_dot, double *logdet, int force_mode);
+
+/* M_hat = 1 + B_0...B_{Nt-1} only (construct_M_hat), out[V*V] row layout of the reference. */
+EPHMC_API int ephmc_construct_M_hat(ephmc_ctx *ctx, const double *x, double *M_hat_out);
+
+/* log|det| and in-place inverse of a V x V matrix (logDetM_and_inv_M_hat):
+ * M is overwritten by its inverse; pivots (1-based, LAPACK convention) are
+ * written to ipiv if not NULL (host).  Returns status; *logdet and *sign out. */
+EPHMC_API int ephmc_logdet_inverse(ephmc_ctx *ctx, double *M, int *ipiv, double *logdet, int *sign);
+
+/* Copy of the most recent M_hat^-1 (row layout of the reference). */
+EPHMC_API int ephmc_ctx_get_inverse(ephmc_ctx *ctx, double *out);
+
+/* Elapsed device milliseconds of the phases of the last ephmc_eval
+ * (M_hat, LU, force), measured with CUDA events on the context stream. */
+EPHMC_API int ephmc_ctx_last_timings(const ephmc_ctx *ctx, float *ms_mhat, float *ms_lu, float *ms_force);
+
+/* Context over a caller-supplied neighbour table (12*ns entries in the layout
+ * of construct_triangular); every site must be the forward neighbour of
+ * exactly one site per link direction.  Used by the drop-in surface, whose
+ * functions receive nnt rather than L1, L2. */
+EPHMC_API int ephmc_ctx_create_nnt(ephmc_ctx **out, const unsigned *nnt, unsigned ns, unsigned nt,
+                         const double t[3], const double kappa[3], double mu, double omega,
+                         unsigned flavors, const ephmc_flags *flags, int device);
+EPHMC_API int ephmc_ctx_set_flags(ephmc_ctx *ctx, const ephmc_flags *flags);
+
+/* ------------------------------------------------------------------ phonon side */
+/* Exact harmonic flow of every Matsubara mode for time h, x and p in place
+ * (evolve_bosons, simulation/organic_bosons.c:126-150). */
+EPHMC_API int ephmc_fa_evolve(ephmc_ctx *ctx, double *x, double *p, double h);
+/* p holds N(0,1) normals (drawn by the caller's MT19937-64 stream as
+ * random_vector does); scaled per mode into Fourier-accelerated momenta
+ * (sample_fourier_momenta, simulation/organic_bosons.c:76-100). */
+EPHMC_API int ephmc_fa_scale_momenta(ephmc_ctx *ctx, double *p);
+/* x holds N(0,1) normals; scaled into a free-phonon sample
+ * (sample_free_bosons, simulation/organic_bosons.c:55-74). */
+EPHMC_API int ephmc_fa_scale_free_bosons(ephmc_ctx *ctx, double *x);
+/* Kinetic energy of p in Fourier space (energy_fourier_momenta, :102-124). */
+EPHMC_API int ephmc_fa_energy(ephmc_ctx *ctx, const double *p, double *energy);
+/* Action -flavors*logdet + energyP + (sum (dx_t)^2/omega + omega sum x^2)/2
+ * (hamilton, simulation/organic_hmc.c:67-84). */
+EPHMC_API int ephmc_hamilton(ephmc_ctx *ctx, const double *x, double logdet, double energyP, double *H);
+
+/* ------------------------------------------------------------------ memory */
+EPHMC_API void *ephmc_alloc(size_t bytes);   /* device memory on the current device */
+EPHMC_API void ephmc_free(void *p);
+EPHMC_API int ephmc_memcpy_h2d(void *dst, const void *src, size_t bytes);
+EPHMC_API int ephmc_memcpy_d2h(void *dst, const void *src, size_t bytes);
+EPHMC_API int ephmc_device_synchronize(void);
+
+/* Cumulative number of kernel launches issued by this library (all contexts). */
+EPHMC_API unsigned long long ephmc_launch_count(void);
+/* CUDA-core FMA throughput of the current device in TFLOP/s (fp64 != 0: FP64,
+ * else FP32), from a dependent-chain FMA probe; the roofline denominator for
+ * the stencil kernels. */
+EPHMC_API int ephmc_measure_fma_peak(int fp64, float *tflops);
+
+/* Library version string. */
+EPHMC_API const char *ephmc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

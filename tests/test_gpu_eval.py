@@ -1,0 +1,193 @@
+"""GPU parity: libephmc_cuda.so against the reference's golden vectors.
+
+Tolerances are anchored on the reference's own reproducibility: every fixture
+stores the spread between the reference run with 1 and with N OpenBLAS
+threads (the LU reduction order is the only thread-dependent step), and the
+force is required to agree to max(1e-10, 10 x that spread) in max-norm
+relative error.  M_hat is required bit-identical: the slice kernels sum the
+stencil in the reference's order.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, model_from_golden
+
+pytestmark = pytest.mark.gpu
+
+WELL = ["small_L6_Nt64", "rect_L4x3_Nt16", "odd_L5x6_Nt12", "tiny_L2x2_Nt4", "line_L1x4_Nt5",
+        "single_slice_L3x3_Nt1"]
+
+
+def ctx_for(g):
+    import ephmc
+    return ephmc.Context(int(g["l1"]), int(g["l2"]), int(g["nt"]), np.array(g["t"]), np.array(g["kappa"]),
+                         float(g["mu"]), float(g["omega"]), int(g["flavors"]))
+
+
+def force_tol(g, n=0):
+    return max(1e-10, 10 * float(np.atleast_1d(g["force_spread_max"])[n]))
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("name", WELL)
+def test_M_hat_bit_identical(gpu, restated, name):
+    g = golden(f"eval_{name}.npz")
+    m = model_from_golden(g)
+    with ctx_for(g) as ctx:
+        for n, seed in enumerate(g["seeds"]):
+            x = restated.random_x(int(seed), m.dim)
+            M = ctx.construct_M_hat(x)
+            assert np.array_equal(M, g["M_hat"][n])
+
+
+@pytest.mark.parametrize("mode", ["reference", "adjoint"])
+@pytest.mark.parametrize("name", WELL)
+def test_eval_fp64_matches_reference(gpu, restated, name, mode):
+    g = golden(f"eval_{name}.npz")
+    m = model_from_golden(g)
+    with ctx_for(g) as ctx:
+        for n, seed in enumerate(g["seeds"]):
+            x = restated.random_x(int(seed), m.dim)
+            ld, pd = ctx.eval(x, mode=mode)
+            assert abs(ld - g["logdet"][n]) <= 1e-12 * abs(g["logdet"][n]) + 1e-13
+            assert rel(pd, g["force"][n]) <= force_tol(g, n), (mode, rel(pd, g["force"][n]))
+            if mode == "reference":
+                Mi = ctx.inverse()
+                assert rel(Mi, g["M_inv"][n]) <= max(1e-10, 10 * float(g["minv_spread_max"][n]))
+
+
+@pytest.mark.parametrize("name", WELL)
+def test_eval_mixed_error_is_bounded(gpu, restated, name):
+    """FP64 M_hat/LU/logdet, FP32 force sweep: log det exact to FP64, force
+    error stated against the FP64 force (see DESIGN.md for its origin)."""
+    g = golden(f"eval_{name}.npz")
+    m = model_from_golden(g)
+    with ctx_for(g) as ctx:
+        x = restated.random_x(int(g["seeds"][0]), m.dim)
+        ld, pd = ctx.eval(x, mode="mixed")
+        assert abs(ld - g["logdet"][0]) <= 1e-12 * abs(g["logdet"][0]) + 1e-13
+        assert rel(pd, g["force"][0]) <= 1e-4
+
+
+def test_mid_size_reference_and_adjoint(gpu, restated):
+    g = golden("eval_mid_L16_Nt64.npz")
+    m = model_from_golden(g)
+    x = restated.random_x(1, m.dim)
+    with ctx_for(g) as ctx:
+        for mode in ("reference", "adjoint"):
+            ld, pd = ctx.eval(x, mode=mode)
+            assert abs(ld - g["logdet"][0]) <= 1e-12 * abs(g["logdet"][0])
+            assert rel(pd, g["force"][0]) <= force_tol(g), mode
+        ld, pd = ctx.eval(x, mode="mixed")
+        assert abs(ld - g["logdet"][0]) <= 1e-12 * abs(g["logdet"][0])
+        assert rel(pd, g["force"][0]) <= 1e-2
+
+
+def test_cfg0_literal_reproduces_reference_behaviour(gpu, restated):
+    """dtau = 0.625: M_hat bit-identical, log det within the reference's own
+    spread, negative determinant reported as a warning (the reference prints)."""
+    g = golden("eval_cfg0_L6_Nt16_beta10.npz")
+    m = model_from_golden(g)
+    x = restated.random_x(1, m.dim)
+    with ctx_for(g) as ctx:
+        assert np.array_equal(ctx.construct_M_hat(x), g["M_hat"][0])
+        ld, _ = ctx.eval(x, mode="reference")
+        assert abs(ld - g["logdet"][0]) <= 5e-3 * abs(g["logdet"][0])
+
+
+def test_lu_against_numpy(gpu):
+    import ephmc
+    rng = np.random.default_rng(0)
+    for V, (l1, l2) in ((36, (6, 6)), (256, (16, 16)), (1024, (32, 32))):
+        A = rng.standard_normal((V, V)) + 3 * np.eye(V)
+        with ephmc.Context(l1, l2, 1, [0.1, 0.1, 0.1], [0, 0, 0], -1.0, 0.1) as ctx:
+            M = A.copy()
+            ld, sign, ipiv = ctx.logdet_inverse(M)
+            s_np, ld_np = np.linalg.slogdet(A.T)  # LAPACK view is the transpose
+            assert abs(ld - ld_np) <= 1e-11 * abs(ld_np)
+            assert sign == int(s_np)
+            # memory holds the inverse in both row- and column-major views
+            assert np.max(np.abs(M - np.linalg.inv(A))) <= 1e-10 * np.max(np.abs(np.linalg.inv(A)))
+            import scipy.linalg as sl
+            _, piv = sl.lu_factor(A.T)
+            assert np.array_equal(ipiv - 1, piv)
+
+
+def test_lu_singular_reports_status(gpu):
+    import ephmc
+    V = 16
+    A = np.random.default_rng(1).standard_normal((V, V))
+    A[5, :] = 0.0  # column 5 in the LAPACK view
+    with ephmc.Context(4, 4, 1, [0.1, 0.1, 0.1], [0, 0, 0], -1.0, 0.1) as ctx:
+        with pytest.raises(ephmc.EphmcError) as e:
+            ctx.logdet_inverse(A.copy())
+        assert e.value.status == 4
+
+
+def test_device_pointers_match_host_pointers(gpu, restated):
+    import torch
+    g = golden("eval_small_L6_Nt64.npz")
+    m = model_from_golden(g)
+    x = restated.random_x(2, m.dim)
+    with ctx_for(g) as ctx:
+        ld_h, pd_h = ctx.eval(x, mode="adjoint")
+        xd = torch.from_numpy(x).cuda()
+        pdd = torch.empty_like(xd)
+        ld_d, _ = ctx.eval(xd, pdd, mode="adjoint")
+        torch.cuda.synchronize()
+        assert ld_h == ld_d
+        assert np.allclose(pdd.cpu().numpy(), pd_h, rtol=0, atol=1e-13 * np.max(np.abs(pd_h)))
+
+
+def test_fa_and_action_match_reference(gpu, restated):
+    import ephmc
+    g = golden("fa_bosons.npz")
+    for (L, nt) in ((4, 16), (6, 64), (3, 5)):
+        tag = f"L{L}_Nt{nt}"
+        om = float(g[f"{tag}_omega"])
+        with ephmc.Context(L, L, nt, [0.1, 0.1, 0.1], [0.01, 0.01, 0.01], -1.0, om) as ctx:
+            x, p = g[f"{tag}_x"].copy(), g[f"{tag}_p"].copy()
+            ctx.fa_evolve(x, p, 0.3)
+            assert np.allclose(x, g[f"{tag}_x_evolved"], rtol=0, atol=1e-12)
+            assert np.allclose(p, g[f"{tag}_p_evolved"], rtol=0, atol=1e-12)
+            pm = restated.random_x(31, 3 * L * L * nt)
+            ctx.fa_scale_momenta(pm)
+            assert np.allclose(pm, g[f"{tag}_p_sampled_seed31"], rtol=0, atol=1e-12)
+            e = ctx.fa_energy(pm)
+            assert abs(e - float(g[f"{tag}_energy_of_p_sampled"])) <= 1e-12 * abs(e)
+            xf = restated.random_x(41, 3 * L * L * nt)
+            ctx.fa_scale_free_bosons(xf)
+            assert np.allclose(xf, g[f"{tag}_x_free_seed41"], rtol=0, atol=1e-12)
+            h = ctx.hamilton(g[f"{tag}_x"], 1.5, 2.5)
+            assert abs(h - float(g[f"{tag}_hamilton_x"])) <= 1e-12 * abs(h)
+
+
+def test_cfg1_fifty_configurations(gpu, restated):
+    """32x32, Nt = 64, beta = 20: the 50 fixed configurations of the metric's
+    validation set (seeds 1..50): log det, action and sampled force entries in
+    the reference algorithm; full force of seed 1 in all three algorithms."""
+    import os
+    from conftest import GOLDEN
+    path = os.path.join(GOLDEN, "eval_cfg1_L32_Nt64.npz")
+    if not os.path.exists(path):
+        pytest.skip("cfg1 fixture not generated")
+    g = np.load(path)
+    m = model_from_golden(g)
+    tol = max(1e-10, 10 * float(np.max(g["force_spread_max"])))
+    with ctx_for(g) as ctx:
+        for n, seed in enumerate(g["seeds"]):
+            x = restated.random_x(int(seed), m.dim)
+            ld, pd = ctx.eval(x, mode="reference")
+            assert abs(ld - g["logdet"][n]) <= 1e-12 * abs(g["logdet"][n]), seed
+            H = ctx.hamilton(x, ld, 0.0)
+            assert abs(H - g["hamilton"][n]) <= 1e-12 * abs(g["hamilton"][n]), seed
+            samp = pd[g["sample_idx"]]
+            assert np.max(np.abs(samp - g["force_sample"][n])) <= tol * np.max(np.abs(pd)), seed
+            assert abs(np.linalg.norm(pd) - g["force_norm"][n]) <= tol * g["force_norm"][n]
+        x = restated.random_x(1, m.dim)
+        for mode in ("reference", "adjoint"):
+            ld, pd = ctx.eval(x, mode=mode)
+            assert rel(pd, g["force_seed1"]) <= tol, mode
