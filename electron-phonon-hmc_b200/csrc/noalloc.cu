@@ -1,0 +1,108 @@
+// Log det + inverse that allocates nothing: the LU's workspace lives in a
+// file-scope device array instead of buffers from cudaMalloc.
+//
+// For callers whose device memory belongs to someone else -- a framework's
+// caching allocator or a pool sized once at start-up -- or who must not
+// allocate after initialisation: for them a cudaMalloc inside the library
+// either fails or takes memory the owner has already accounted for.  They pass
+// the matrix (device memory they own) and get it back inverted, with log|det|,
+// the sign and the pivots; the library touches no allocator.
+//
+// Limits and sharing:
+//  * n <= kNoAllocMaxN (256): the workspace is the inverse buffer (n*n doubles),
+//    U's diagonal (n+2 doubles), the pivots (n ints) and a status flag, about
+//    0.5 MB, held by every GPU that loads the library until the process exits;
+//  * all calls share that one array and it keeps the last call's contents;
+//    calls that overlap on the GPU (different streams or threads, or another
+//    device context sharing the GPU) race on it and must be serialised by the
+//    caller;
+//  * the first call on a device looks up the array's device address
+//    (cudaGetSymbolAddress, with that device current) and caches it; make
+//    that first call before any stream capture.
+#include "ephmc_internal.cuh"
+
+#include <mutex>
+
+namespace {
+
+constexpr unsigned kNoAllocMaxN = 256;
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kOffX = 0;
+constexpr size_t kOffDiag = kOffX + align256(sizeof(double) * kNoAllocMaxN * kNoAllocMaxN);
+constexpr size_t kOffIpiv = kOffDiag + align256(sizeof(double) * (kNoAllocMaxN + 2));
+constexpr size_t kOffInfo = kOffIpiv + align256(sizeof(int) * kNoAllocMaxN);
+constexpr size_t kNoAllocBytes = kOffInfo + align256(sizeof(int) * 2);
+
+// Host code must not take this symbol's address directly (that is a host-side
+// stand-in); the device address comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+unsigned char *g_addr[kMaxDevices] = {nullptr};
+
+int scratch_for_current_device(unsigned char **out) {
+    int dev = 0;
+    EPHMC_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        ephmc::set_status(EPHMC_ERR_UNSUPPORTED, "device ordinal beyond the no-alloc table");
+        return EPHMC_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return ephmc::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_addr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_addr[dev];
+    return EPHMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+EPHMC_API int ephmc_logdet_inverse_noalloc(double *M, unsigned n, double *logdet, int *sign, int *ipiv,
+                                           void *stream) {
+    ephmc::clear_status();
+    if (!M || n == 0) {
+        ephmc::set_status(EPHMC_ERR_ARG, "ephmc_logdet_inverse_noalloc: null matrix or n == 0");
+        return EPHMC_ERR_ARG;
+    }
+    if (n > kNoAllocMaxN) {
+        ephmc::set_status(EPHMC_ERR_ARG,
+                          "ephmc_logdet_inverse_noalloc: n exceeds the 256 x 256 limit of the static workspace");
+        return EPHMC_ERR_ARG;
+    }
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, M) != cudaSuccess ||
+        (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)) {
+        cudaGetLastError();
+        ephmc::set_status(EPHMC_ERR_ARG, "ephmc_logdet_inverse_noalloc: M must be device memory");
+        return EPHMC_ERR_ARG;
+    }
+    unsigned char *base = nullptr;
+    int rc = scratch_for_current_device(&base);
+    if (rc != EPHMC_OK) return rc;
+    ephmc::LUWork w;
+    w.V = (int)n;
+    w.X = reinterpret_cast<double *>(base + kOffX);
+    w.diag = reinterpret_cast<double *>(base + kOffDiag);
+    w.ipiv = reinterpret_cast<int *>(base + kOffIpiv);
+    w.info = reinterpret_cast<int *>(base + kOffInfo);  // zeroed by the factorisation itself
+    int sg = 1;
+    double ld = 0;
+    rc = ephmc::lu_logdet_inverse(M, w, &ld, &sg, ipiv, static_cast<cudaStream_t>(stream));
+    if (logdet) *logdet = ld;
+    if (sign) *sign = sg;
+    if (rc != EPHMC_OK) {
+        ephmc::set_status(rc, rc == EPHMC_ERR_SINGULAR ? "zero pivot" : nullptr);
+        return rc;
+    }
+    const cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return ephmc::cuda_fail(e, "cudaStreamSynchronize");
+    return EPHMC_OK;
+}
+
+}  // extern "C"

@@ -132,6 +132,19 @@ EPHMC_API int ephmc_construct_M_hat(ephmc_ctx *ctx, const double *x, double *M_h
  * written to ipiv if not NULL (host).  Returns status; *logdet and *sign out. */
 EPHMC_API int ephmc_logdet_inverse(ephmc_ctx *ctx, double *M, int *ipiv, double *logdet, int *sign);
 
+/* No counterpart in the reference.  log|det| and in-place inverse of a device
+ * matrix M (n x n, n <= 256) that allocates nothing: for callers whose device
+ * memory is owned by a framework's caching allocator or by a pool sized at
+ * start-up, or who must not allocate after initialisation.  The LU workspace
+ * is a file-scope device array (about 0.5 MB, held by every GPU that loads the
+ * library until exit), shared by all calls and left holding the last call's
+ * data: calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on each device looks up the array's address and
+ * should come before any stream capture.  n > 256 returns EPHMC_ERR_ARG.
+ * ipiv (host, may be NULL) receives 1-based pivots; stream may be NULL. */
+EPHMC_API int ephmc_logdet_inverse_noalloc(double *M, unsigned n, double *logdet, int *sign, int *ipiv,
+                                           void *stream);
+
 /* Copy of the most recent M_hat^-1 (row layout of the reference). */
 EPHMC_API int ephmc_ctx_get_inverse(ephmc_ctx *ctx, double *out);
 
