@@ -178,6 +178,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--paths", default="mixed,adjoint,reference")
+    ap.add_argument("--profile", action="store_true",
+                    help="run only warm-up + timed evaluations of --paths (for ncu); print nothing")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -245,6 +247,11 @@ def main():
                          "clocks": sampler.summary() if sampler else None}
         phase[path] = {"mhat_ms": statistics.median(p[0] for p in ph), "lu_ms": statistics.median(p[1] for p in ph),
                        "force_ms": statistics.median(p[2] for p in ph)}
+
+    if args.profile:
+        # profiling mode (under ncu): only the warm-up and timed evaluations above
+        ctx.close()
+        return 0
 
     head = "mixed" if "mixed" in results else paths[0]
     r = results[head]
