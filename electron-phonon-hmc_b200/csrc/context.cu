@@ -207,9 +207,9 @@ int stage_out(ephmc_ctx *c, double *user, const double *devbuf, size_t n) {
     return EPHMC_OK;
 }
 
-// M_hat (or, with a stack, sweep 1 of the adjoint) into c->M
-int build_M_hat(ephmc_ctx *c, const double *x, void *stack, bool stack_float) {
-    SliceJob j = job(nullptr, c->M, (int)c->nt - 1, (int)c->nt, -1, 0, kPairs, 1);
+// M_hat (or, with a stack, sweep 1 of the adjoint) into dst (default c->M)
+int build_M_hat(ephmc_ctx *c, const double *x, void *stack, bool stack_float, double *dst = nullptr) {
+    SliceJob j = job(nullptr, dst ? dst : c->M, (int)c->nt - 1, (int)c->nt, -1, 0, kPairs, 1);
     j.add_identity = !(c->flags.zero_filling || c->flags.single_particle);
     j.stack = stack;
     j.stack_off = -1;
@@ -236,12 +236,14 @@ int factor(ephmc_ctx *c, double *logdet, int *ipiv_host) {
 // construct_all_QM1P (simulation/organic_dense_matrix.c:311-381) as batched launches:
 // per halving pass, every spawned copy (P side, on columns) in one launch, then
 // every Q-side extension (on rows) in one launch.
-int all_G(ephmc_ctx *c, const double *x) {
+int all_G(ephmc_ctx *c, const double *x, const double *Minv = nullptr, double *Gbase = nullptr,
+          int *perm_out = nullptr) {
     const unsigned nt = c->nt;
     const size_t VV = (size_t)c->V * c->V;
+    double *G = Gbase ? Gbase : c->G;
     int rc;
-    if (!c->flags.single_particle) rc = launch_copy(c->G, c->M, VV, c->stream);
-    else rc = launch_identity(c->G, (int)c->V, c->stream);
+    if (!c->flags.single_particle) rc = launch_copy(G, Minv ? Minv : c->M, VV, c->stream);
+    else rc = launch_identity(G, (int)c->V, c->stream);
     if (rc) return rc;
     std::vector<unsigned> from_q(nt, 0), from_p(nt, 0);
     unsigned left = nt - 1;
@@ -252,9 +254,9 @@ int all_G(ephmc_ctx *c, const double *x) {
         for (int i = (int)nt - 1; i >= 0; --i) {
             if (!(i == 0 || from_q[i] || from_p[i])) continue;
             const unsigned j = (unsigned)i + chunk;
-            double *Gi = c->G + (size_t)i * VV;
+            double *Gi = G + (size_t)i * VV;
             if (j < nt && from_q[j] == 0 && from_p[j] == 0) {
-                spawn.push_back(job(Gi, c->G + (size_t)j * VV, (int)from_p[i], (int)chunk, +1, 0, kPairs, 1));
+                spawn.push_back(job(Gi, G + (size_t)j * VV, (int)from_p[i], (int)chunk, +1, 0, kPairs, 1));
                 from_q[j] = from_q[i];
                 from_p[j] = from_p[i] + chunk;
             }
@@ -272,6 +274,11 @@ int all_G(ephmc_ctx *c, const double *x) {
                                                         (int)ext.size(), c->stream)))
             return rc;
     }
+    if (perm_out)
+        for (unsigned i = 0; i < nt; ++i) {
+            perm_out[i] = (int)from_q[i];
+            perm_out[nt + i] = (int)from_p[i];
+        }
     if (left != 0) return ret(EPHMC_ERR_UNSUPPORTED, "log-depth sharing left slices unaccounted");
     for (unsigned i = 0; i < nt; ++i)
         if (from_q[i] + from_p[i] != nt - 1) return ret(EPHMC_ERR_UNSUPPORTED, "G_t bookkeeping mismatch");
@@ -279,16 +286,17 @@ int all_G(ephmc_ctx *c, const double *x) {
 }
 
 // refine_QM1P + force contraction for every slice, in batches of refine_batch slices
-int refine_all(ephmc_ctx *c, const double *x, double logdet) {
+int refine_all(ephmc_ctx *c, const double *x, double logdet, const double *Gbase = nullptr) {
     const unsigned nt = c->nt;
     const size_t VV = (size_t)c->V * c->V;
     const int nb = c->refine_batch;
+    const double *G = Gbase ? Gbase : c->G;
     int rc;
     for (unsigned t0 = 0; t0 < nt; t0 += nb) {
         const int cnt = (int)std::min<unsigned>(nb, nt - t0);
         std::vector<SliceJob> cols, rows;
         for (int b = 0; b < cnt; ++b) {
-            const double *Gt = c->G + (size_t)(t0 + b) * VV;
+            const double *Gt = G + (size_t)(t0 + b) * VV;
             // pair 0: X_0 = G F_>0 -> pair 1 on columns (transpose, apply_exp revert, :410-413)
             cols.push_back(job(Gt, c->A + (size_t)b * VV, (int)(t0 + b), 1, 1, 1, 2, 1));
             // pair 1: X_1 = F_<1 G -> pair 0 on rows (apply_exp forward, :408)
@@ -305,6 +313,100 @@ int refine_all(ephmc_ctx *c, const double *x, double logdet) {
                                      c->flags.single_particle, logdet, c->force, c->stream)))
             return rc;
     }
+    return EPHMC_OK;
+}
+
+// Full-matrix refine_QM1P of one V x V matrix G (device) for slice t, in place
+// (simulation/organic_dense_matrix.c:383-442), on the context's work buffers.
+int refine_full(ephmc_ctx *c, const double *x, double *G, unsigned t) {
+    const size_t VV = (size_t)c->V * c->V;
+    const double *xs = x + (size_t)t * 3 * c->V;
+    double *w0 = c->work, *w1 = w0 + VV, *w2 = w1 + VV, *w3 = w2 + VV;
+    const int V = (int)c->V;
+    int rc;
+    for (int p = 0; p < kPairs; ++p) {
+        // pair 0: X_0 = G with pair 1 on columns; pair 1: X_1 = G with pair 0 on rows
+        SliceJob j = (p == 0) ? job(G, w0, 0, 1, 1, 1, 2, 1) : job(G, w0, 0, 1, 1, 0, 1, 1);
+        std::vector<SliceJob> v{j};
+        if ((rc = upload_jobs(c, v, c->jobs))) return rc;
+        if ((rc = launch_slices<double, double, double>(p == 0 ? Axis::Cols : Axis::Rows, xs, c->c, c->lat,
+                                                        c->jobs, 1, c->stream)))
+            return rc;
+        if ((rc = launch_stencil(xs, c->c, c->lat, w0, w1, V, true, false, c->stream))) return rc;   // X H
+        if ((rc = launch_stencil(xs, c->c, c->lat, w0, w2, V, false, false, c->stream))) return rc;  // H X
+        if ((rc = launch_combine_refine(w3, w0, w2, w1, VV, c->c.a_lin[p], c->c.a_quad[p], p == 0, c->stream)))
+            return rc;
+    }
+    return launch_copy(G, w3, VV, c->stream);
+}
+
+// log det step of logDetM_and_inv_M_hat on c->M: single_particle takes log(trace M)
+// (simulation/organic_dense_matrix.c:550-551), otherwise the LU.
+int logdet_step(ephmc_ctx *c, double *ld, int *ipiv_host) {
+    if (c->flags.schur_form_inv) return ret(EPHMC_ERR_UNSUPPORTED, "SCHUR_FORM_INV (dgees) is not implemented");
+    if (c->flags.single_particle) {
+        double *out = c->scratch + c->scratch_n - 8;
+        int rc = launch_trace(c->M, (int)c->V, out, c->stream);
+        if (rc) return rc;
+        double tr = 0;
+        EPHMC_CUDA(cudaMemcpyAsync(&tr, out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+        *ld = std::log(tr);
+        c->last_logdet = *ld;
+        c->have_inverse = false;
+        return EPHMC_OK;
+    }
+    return factor(c, ld, ipiv_host);
+}
+
+// force() (simulation/organic_hmc.c:86-134) from the inverse Minv (device), into c->force.
+// mode: reference algorithm or adjoint (FP64 / mixed); flags CONSTANT_FORCE,
+// SINGLE_PARTICLE and NO_FOURIER_ACC as the reference.
+int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet, int mode, bool have_qstack) {
+    const ephmc_flags &f = c->flags;
+    const size_t VV = (size_t)c->V * c->V;
+    int rc;
+    if (f.schur_form_inv) return ret(EPHMC_ERR_UNSUPPORTED, "SCHUR_FORM_INV (dgees) is not implemented");
+    if (f.constant_force) {
+        // construct_QM1P(time = 0): Q_0 M^-1, refined at slice 0, used for every slice (:92-105, :267-309)
+        double *G0 = c->G;
+        if (!f.single_particle) rc = launch_copy(G0, Minv, VV, c->stream);
+        else rc = launch_identity(G0, (int)c->V, c->stream);
+        if (rc) return rc;
+        if (c->nt > 1) {
+            std::vector<SliceJob> v{job(G0, G0, (int)c->nt - 1, (int)c->nt - 1, -1, 0, kPairs, 1)};
+            if ((rc = upload_jobs(c, v, c->jobs))) return rc;
+            if ((rc = launch_slices<double, double, double>(Axis::Rows, xd, c->c, c->lat, c->jobs, 1, c->stream)))
+                return rc;
+        }
+        if ((rc = refine_full(c, xd, G0, 0))) return rc;
+        if ((rc = launch_contract_full(G0, c->c, c->lat, (int)c->nt, c->flavors, f.schur_form_inv, f.single_particle,
+                                       std::exp(-logdet), c->force, c->stream)))
+            return rc;
+    } else if (mode == EPHMC_FORCE_REFERENCE) {
+        if ((rc = all_G(c, xd, Minv))) return rc;
+        if ((rc = refine_all(c, xd, logdet))) return rc;
+    } else {
+        const bool mixed = mode == EPHMC_FORCE_MIXED;
+        if (!have_qstack)
+            if ((rc = build_M_hat(c, xd, c->qstack, mixed, c->work))) return rc;
+        const double *y0 = Minv;
+        if (f.single_particle) {  // G_t = Q_t P_t: y(0) rows are the identity
+            if ((rc = launch_identity(c->work, (int)c->V, c->stream))) return rc;
+            y0 = c->work;
+        }
+        if (!mixed)
+            rc = launch_adjoint_sweep<double, double>(xd, c->c, c->lat, static_cast<const double *>(c->qstack), y0,
+                                                      (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
+                                                      c->stream);
+        else
+            rc = launch_adjoint_sweep<float, float>(xd, c->c, c->lat, static_cast<const float *>(c->qstack), y0,
+                                                    (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
+                                                    c->stream);
+        if (rc) return rc;
+    }
+    if (f.no_fourier_acc)
+        return launch_boson_force(xd, c->force, c->omega, 3 * (int)c->V, (int)c->nt, false, c->stream);
     return EPHMC_OK;
 }
 
@@ -365,8 +467,9 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(c->device);
-    void *bufs[] = {c->x, c->force, c->M, c->G, c->A, c->B, c->qstack, c->jobs, c->lat.ev_src, c->lat.ev_fac,
-                    c->lat.nbr, c->scratch};
+    void *bufs[] = {c->x,         c->force,        c->M,          c->G,        c->A,
+                    c->B,         c->qstack,       c->jobs,       c->lat.ev_src, c->lat.ev_fac,
+                    c->lat.nbr,   c->lat.rev,      c->scratch,    c->work,     c->cc_part};
     for (void *b : bufs)
         if (b) cudaFree(b);
     lu_free(c->lu);
@@ -431,6 +534,9 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     ALLOC(c->lat.ev_src, sizeof(int) * 6 * V);
     ALLOC(c->lat.ev_fac, sizeof(int) * 6 * V);
     ALLOC(c->lat.nbr, sizeof(int) * 3 * V);
+    ALLOC(c->lat.rev, sizeof(int) * 3 * V);
+    ALLOC(c->work, sizeof(double) * VV * 4);
+    ALLOC(c->cc_part, sizeof(double) * (size_t)nt * V * 9);
     ALLOC(c->x, sizeof(double) * dim);
     ALLOC(c->force, sizeof(double) * dim);
     ALLOC(c->M, sizeof(double) * VV);
@@ -449,6 +555,12 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     cudaMemcpy(c->lat.ev_src, es.data(), sizeof(int) * 6 * V, cudaMemcpyHostToDevice);
     cudaMemcpy(c->lat.ev_fac, ef.data(), sizeof(int) * 6 * V, cudaMemcpyHostToDevice);
     cudaMemcpy(c->lat.nbr, nb.data(), sizeof(int) * 3 * V, cudaMemcpyHostToDevice);
+    {
+        std::vector<int> rv(3 * (size_t)V, 0);
+        for (unsigned k = 0; k < 3; ++k)
+            for (unsigned i = 0; i < V; ++i) rv[(size_t)k * V + nb[(size_t)k * V + i]] = (int)i;
+        cudaMemcpy(c->lat.rev, rv.data(), sizeof(int) * 3 * V, cudaMemcpyHostToDevice);
+    }
     for (auto &e : c->ev)
         if (cudaEventCreate(&e) != cudaSuccess) {
             ephmc_ctx_destroy(c);
@@ -557,35 +669,22 @@ int ephmc_eval(ephmc_ctx *c, const double *x, double *p_dot, double *logdet, int
     if (!c || !x) return ret(EPHMC_ERR_ARG, "ephmc_eval");
     if (mode < EPHMC_FORCE_REFERENCE || mode > EPHMC_FORCE_MIXED) return ret(EPHMC_ERR_ARG, "force mode");
     const ephmc_flags &f = c->flags;
-    if (f.schur_form_inv || f.constant_force || f.single_particle || f.zero_filling)
-        return ret(EPHMC_ERR_UNSUPPORTED, "flag not implemented on the GPU path");
+    if (f.schur_form_inv) return ret(EPHMC_ERR_UNSUPPORTED, "SCHUR_FORM_INV (dgees) is not implemented");
     EPHMC_CUDA(cudaSetDevice(c->device));
     const size_t dim = (size_t)c->nt * c->V * 3;
     const double *xd = nullptr;
     int rc;
     if ((rc = stage_in(c, x, c->x, dim, &xd))) return ret(rc);
     EPHMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
-    const bool adj = mode != EPHMC_FORCE_REFERENCE;
+    const bool adj = mode != EPHMC_FORCE_REFERENCE && !f.constant_force;
     const bool mixed = mode == EPHMC_FORCE_MIXED;
     if ((rc = build_M_hat(c, xd, adj ? c->qstack : nullptr, mixed))) return ret(rc);
     EPHMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
     double ld = 0;
-    rc = factor(c, &ld, nullptr);
+    rc = logdet_step(c, &ld, nullptr);
     if (rc) return ret(rc, rc == EPHMC_ERR_SINGULAR ? "zero pivot" : nullptr);
     EPHMC_CUDA(cudaEventRecord(c->ev[2], c->stream));
-    if (!adj) {
-        if ((rc = all_G(c, xd))) return ret(rc);
-        if ((rc = refine_all(c, xd, ld))) return ret(rc);
-    } else if (!mixed) {
-        rc = launch_adjoint_sweep<double, double>(xd, c->c, c->lat, static_cast<const double *>(c->qstack), c->M,
-                                                  (int)c->nt, c->flavors, f.single_particle, ld, c->force,
-                                                  c->stream);
-        if (rc) return ret(rc);
-    } else {
-        rc = launch_adjoint_sweep<float, float>(xd, c->c, c->lat, static_cast<const float *>(c->qstack), c->M,
-                                                (int)c->nt, c->flavors, f.single_particle, ld, c->force, c->stream);
-        if (rc) return ret(rc);
-    }
+    if ((rc = force_core(c, xd, c->M, ld, mode, adj))) return ret(rc);
     EPHMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
     if ((rc = stage_out(c, p_dot, c->force, dim))) return ret(rc);
     EPHMC_CUDA(cudaStreamSynchronize(c->stream));
@@ -594,6 +693,132 @@ int ephmc_eval(ephmc_ctx *c, const double *x, double *p_dot, double *logdet, int
     cudaEventElapsedTime(&c->t_force, c->ev[2], c->ev[3]);
     if (logdet) *logdet = ld;
     if (!std::isfinite(ld)) return ret(EPHMC_ERR_NONFINITE, "log det not finite");
+    return EPHMC_OK;
+}
+
+// force() given the inverse M_inv (simulation/organic_hmc.c:86-134)
+int ephmc_force(ephmc_ctx *c, const double *x, const double *M_inv, double logdet, double *p_dot, int mode) {
+    clear_status();
+    if (!c || !x || !p_dot) return ret(EPHMC_ERR_ARG, "ephmc_force");
+    if (mode < EPHMC_FORCE_REFERENCE || mode > EPHMC_FORCE_MIXED) return ret(EPHMC_ERR_ARG, "force mode");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t dim = (size_t)c->nt * c->V * 3, VV = (size_t)c->V * c->V;
+    const double *xd = nullptr, *Mi = nullptr;
+    int rc;
+    if ((rc = stage_in(c, x, c->x, dim, &xd))) return ret(rc);
+    if (!c->flags.single_particle && M_inv) {
+        if ((rc = stage_in(c, M_inv, c->M, VV, &Mi))) return ret(rc);
+    } else {
+        Mi = c->M;
+    }
+    if ((rc = force_core(c, xd, Mi, logdet, mode, false))) return ret(rc);
+    if ((rc = stage_out(c, p_dot, c->force, dim))) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    return EPHMC_OK;
+}
+
+// construct_all_QM1P: G_t = Q_t M^-1 P_t for every t into G_out (nt*V*V), bookkeeping
+// (slices taken on the Q side, then on the P side) into perm_out[2*nt] if given
+int ephmc_all_G(ephmc_ctx *c, const double *x, const double *M_inv, double *G_out, int *perm_out) {
+    clear_status();
+    if (!c || !x || !G_out) return ret(EPHMC_ERR_ARG, "ephmc_all_G");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t dim = (size_t)c->nt * c->V * 3, VV = (size_t)c->V * c->V;
+    const double *xd = nullptr, *Mi = c->M;
+    int rc;
+    if ((rc = stage_in(c, x, c->x, dim, &xd))) return ret(rc);
+    if (M_inv && !c->flags.single_particle)
+        if ((rc = stage_in(c, M_inv, c->M, VV, &Mi))) return ret(rc);
+    const bool dev = is_device_ptr(G_out);
+    if ((rc = all_G(c, xd, Mi, dev ? G_out : c->G, perm_out))) return ret(rc);
+    if (!dev) EPHMC_CUDA(cudaMemcpyAsync(G_out, c->G, sizeof(double) * VV * c->nt, cudaMemcpyDeviceToHost, c->stream));
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    return EPHMC_OK;
+}
+
+// refine_QM1P on one matrix G (V*V, in place) for slice t
+int ephmc_refine_G(ephmc_ctx *c, const double *x, double *G, unsigned t) {
+    clear_status();
+    if (!c || !x || !G || t >= c->nt) return ret(EPHMC_ERR_ARG, "ephmc_refine_G");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t dim = (size_t)c->nt * c->V * 3, VV = (size_t)c->V * c->V;
+    const double *xd = nullptr, *Gd = nullptr;
+    int rc;
+    if ((rc = stage_in(c, x, c->x, dim, &xd))) return ret(rc);
+    if ((rc = stage_in(c, G, c->M, VV, &Gd))) return ret(rc);
+    if ((rc = refine_full(c, xd, const_cast<double *>(Gd), t))) return ret(rc);
+    if ((rc = stage_out(c, G, Gd, VV))) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    return EPHMC_OK;
+}
+
+// apply_exp_mu_K_to_M (simulation/organic_dense_matrix.c:209-216): nrows contiguous rows of
+// length V in M get the pair product of one slice (x_slice: 3V fields); revert/stop as the reference
+int ephmc_apply_exp_rows(ephmc_ctx *c, const double *x_slice, double *M, unsigned nrows, int revert, int stop) {
+    clear_status();
+    if (!c || !x_slice || !M || nrows == 0 || nrows > c->V) return ret(EPHMC_ERR_ARG, "ephmc_apply_exp_rows");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t n = (size_t)nrows * c->V;
+    const double *xs = nullptr, *Md = nullptr;
+    int rc;
+    if ((rc = stage_in(c, x_slice, c->x, 3 * (size_t)c->V, &xs))) return ret(rc);
+    if ((rc = stage_in(c, M, c->work, n, &Md))) return ret(rc);
+    const int pb = revert ? kPairs - 1 : 0, pe = revert ? stop : stop, ps = revert ? -1 : 1;
+    if ((revert && pb > pe) || (!revert && pe > pb)) {
+        // the slice kernel propagates whole V x V matrices; nrows < V rows ride in a zero-padded copy
+        double *tmp = c->work + 2 * (size_t)c->V * c->V;
+        if (nrows < c->V) {
+            EPHMC_CUDA(cudaMemsetAsync(tmp, 0, sizeof(double) * (size_t)c->V * c->V, c->stream));
+            EPHMC_CUDA(cudaMemcpyAsync(tmp, Md, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+        }
+        double *target = (nrows < c->V) ? tmp : const_cast<double *>(Md);
+        std::vector<SliceJob> v{job(target, target, 0, 1, 1, pb, pe, ps)};
+        if ((rc = upload_jobs(c, v, c->jobs))) return ret(rc);
+        if ((rc = launch_slices<double, double, double>(Axis::Rows, xs, c->c, c->lat, c->jobs, 1, c->stream)))
+            return ret(rc);
+        if (nrows < c->V)
+            EPHMC_CUDA(cudaMemcpyAsync(const_cast<double *>(Md), tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                       c->stream));
+    }
+    if ((rc = stage_out(c, M, Md, n))) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    return EPHMC_OK;
+}
+
+// out = (mu + K) in on nrows rows (apply_mu_K_to_v / apply_mu_K_to_M, :96-131);
+// add_in: out = in + (mu + K) in (apply_K_plus_1_v, :162-166)
+int ephmc_apply_stencil_rows(ephmc_ctx *c, const double *x_slice, const double *in, double *out, unsigned nrows,
+                             int add_in) {
+    clear_status();
+    if (!c || !x_slice || !in || !out || nrows == 0) return ret(EPHMC_ERR_ARG, "ephmc_apply_stencil_rows");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t n = (size_t)nrows * c->V;
+    if (n > 2 * (size_t)c->V * c->V) return ret(EPHMC_ERR_ARG, "too many rows");
+    const double *xs = nullptr, *ind = nullptr;
+    int rc;
+    if ((rc = stage_in(c, x_slice, c->x, 3 * (size_t)c->V, &xs))) return ret(rc);
+    if ((rc = stage_in(c, in, c->work, n, &ind))) return ret(rc);
+    double *od = is_device_ptr(out) ? out : c->work + 2 * (size_t)c->V * c->V;
+    if ((rc = launch_stencil(xs, c->c, c->lat, ind, od, (int)nrows, false, add_in != 0, c->stream))) return ret(rc);
+    if ((rc = stage_out(c, out, od, n))) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    return EPHMC_OK;
+}
+
+// w = I_k v, the antisymmetric current along link k (apply_current_to_v, :226-249)
+int ephmc_apply_current(ephmc_ctx *c, const double *x_slice, const double *v, double *w, unsigned k) {
+    clear_status();
+    if (!c || !x_slice || !v || !w || k > 2) return ret(EPHMC_ERR_ARG, "ephmc_apply_current");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t V = c->V;
+    const double *xs = nullptr, *vd = nullptr;
+    int rc;
+    if ((rc = stage_in(c, x_slice, c->x, 3 * V, &xs))) return ret(rc);
+    if ((rc = stage_in(c, v, c->work, V, &vd))) return ret(rc);
+    double *wd = is_device_ptr(w) ? w : c->work + V;
+    if ((rc = launch_current(xs, c->c, c->lat, c->lat.rev + (size_t)k * V, vd, wd, (int)k, c->stream))) return ret(rc);
+    if ((rc = stage_out(c, w, wd, V))) return ret(rc);
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
     return EPHMC_OK;
 }
 

@@ -54,6 +54,7 @@ struct LatticeDev {
     int *ev_src = nullptr;
     int *ev_fac = nullptr;
     int *nbr = nullptr;
+    int *rev = nullptr;  // rev[k*V + j]: the site whose link-k neighbour is j
 };
 
 // Host helper: build the event tables; returns EPHMC_OK or EPHMC_ERR_LATTICE.
@@ -97,6 +98,42 @@ template <typename Real, typename QT>
 int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat,
                          const QT *qstack, const double *Minv, int nt, unsigned flavors,
                          int single_particle, double logdet, double *force, cudaStream_t st);
+
+// ---------------------------------------------------------------- drop-in helpers (helpers.cu)
+// out = (mu + K) in on nvec rows (or columns) of V x V matrices, reference order;
+// add_in: out = in + (mu + K) in (apply_K_plus_1_v)
+int launch_stencil(const double *xs, const Couplings &c, const LatticeDev &lat, const double *in, double *out,
+                   int nvec, bool cols, bool add_in, cudaStream_t st);
+int launch_current(const double *xs, const Couplings &c, const LatticeDev &lat, const int *rev_k, const double *v,
+                   double *w, int k, cudaStream_t st);
+int launch_combine_refine(double *G, const double *X, const double *X1, const double *X2, size_t n, double al,
+                          double aq, bool first, cudaStream_t st);
+int launch_matvec(const double *m, const double *x, double *y, int n, bool tr, cudaStream_t st);
+int launch_matmat_rows(const double *m1, const double *m2, double *out, int n, cudaStream_t st);
+int launch_transpose_rect(const double *x, double *y, int n1, int n2, cudaStream_t st);
+int launch_trace(const double *m, int n, double *out_dev, cudaStream_t st);
+int launch_boson_force(const double *x, double *pd, double omega, int ld, int nt, bool overwrite, cudaStream_t st);
+int device_moments(const double *x, size_t n, double *part_dev, double out[2], cudaStream_t st);
+int device_matsubara_norm(const double *x, int ld, int nt, double *part_dev, double *out, cudaStream_t st);
+int launch_phonon_corr(const double *x, int ns, int nt, double *g, cudaStream_t st);
+int launch_add_diag(double *M, int V, double v, cudaStream_t st);
+int launch_contract_full(const double *D, const Couplings &c, const LatticeDev &lat, int nt, unsigned flavors,
+                         int schur, int sp, double spw, double *force, cudaStream_t st);
+int launch_axpy(double *y, const double *x, double a, size_t n, cudaStream_t st);
+int launch_pair_combine(double *v, const double *w, const double *z, double al, double aq, size_t n, cudaStream_t st);
+
+// ---------------------------------------------------------------- drop-in glue (organic_api.cu)
+double dropin_contract_greens(const double *gr, const double *mat, unsigned nn, unsigned tau);
+double dropin_rng_real2();
+void dropin_rng_normals(double *x, unsigned n);
+void dropin_rng_seed(unsigned long long s);
+int dropin_force_mode();
+
+// ---------------------------------------------------------------- measurement (correlator.cu)
+// cc_correlator (simulation/organic_dense_matrix.c:451-524) on device buffers:
+// Minv (V*V), R_t0 (nt*V*V), R_0t (V*V), greens (nt*9, device)
+int cc_correlator_dev(ephmc_ctx *c, const double *x, const double *Minv, double *R_t0, double *R_0t, double *greens,
+                      double logdet);
 
 // ---------------------------------------------------------------- dense helpers
 int launch_copy(double *dst, const double *src, size_t n, cudaStream_t st);
@@ -158,6 +195,8 @@ struct ephmc_ctx {
     bool have_inverse = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     float t_mhat = 0, t_lu = 0, t_force = 0;
+    double *work = nullptr;     // 4 V*V doubles: full-matrix refinement and drop-in staging
+    double *cc_part = nullptr;  // nt * V * 9 doubles: correlator partial sums
     double *scratch = nullptr;  // small device scratch (Fourier mode tables, reductions)
     size_t scratch_n = 0;
 };

@@ -1,26 +1,32 @@
-// FP64 LU with partial pivoting, log|det| and inverse of the fermion matrix.
+// FP64 log|det| and in-place inverse of the fermion matrix by blocked
+// Gauss-Jordan elimination with partial pivoting.
 //
 // Replaces LAPACKE_dgetrf + LAPACKE_dgetri in logDetM_and_inv_M_hat
-// (simulation/organic_dense_matrix.c:580-595).  The matrix is treated
-// column-major exactly as LAPACK does: A(r,c) = M[c*V + r], so a column is a
-// contiguous row of the reference's array.  Pivoting picks the first row of
-// largest magnitude (LAPACK idamax); log|det| = sum log|U_ii| and the sign
-// from the diagonal signs and the pivot parity (:582-589).
+// (simulation/organic_dense_matrix.c:580-595).  The matrix is seen
+// column-major as LAPACK sees it: A(r,c) = M[c*V + r], so column c is the
+// contiguous row c of the reference's array.  Pivot rows are chosen among the
+// rows not yet used as pivots exactly as dgetrf chooses them (largest
+// magnitude, first on ties), so the pivot sequence and U's diagonal are those
+// of the LU factorisation: log|det| = sum log|U_ii|, the sign from the
+// diagonal signs and the pivot parity (:582-589), pivots reported 1-based.
 //
-// Right-looking blocked factorisation, panel width nb:
-//   k_lu_panel  one 1024-thread CTA factors the nb-column panel held in shared
-//               memory (argmax by warp shuffles + one shared-memory round);
-//   k_lu_trail  every CTA owns CB trailing columns in shared memory, applies
-//               the panel's row interchanges, the unit-lower triangular solve
-//               for its U12 block and the rank-nb update of its rows below;
-//               left-of-panel columns only take the interchanges.
-// Inverse: A^-1 = U^-1 L^-1 P; k_lu_inverse gives each CTA NR columns of the
-// identity (permuted by P), solves L then U in 32-row blocks, writes the
-// columns of A^-1 (column-major, i.e. rows of the reference's array).
+// Per panel of nb columns p (rows P = p, others O):
+//   k_gj_panel   one 1024-thread CTA, every thread owns one row of the panel
+//                in registers: LU with partial pivoting of rows >= j0 (argmax by
+//                __reduce_max_sync on the bit pattern of |a|), then
+//                D^-1 = U11^-1 L11^-1 and the new panel columns
+//                (rows P: D^-1; rows below: -L21 L11^-1; rows above: -C D^-1);
+//   k_gj_update  every CTA owns CB other columns in shared memory: applies the
+//                panel's interchanges, sets rows P to D^-1 A(P, col) and
+//                updates the other rows A(O, col) -= K A(P, col) with
+//                K = A(O, p) D^-1 = -(new panel columns).
+// After the last panel the interchanges are undone as column permutations.
+// 2V^3 flops in V/nb rank-nb updates over the full matrix (GEMM-shaped, L2
+// resident at V = 1024), with no separate triangular-solve phase.
 #include "ephmc_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
-#include <vector>
 
 namespace ephmc {
 
@@ -28,255 +34,288 @@ namespace {
 
 constexpr int kPanelThreads = 1024;
 
-__device__ __forceinline__ void better(double &bv, int &bi, double v, int i) {
-    // larger magnitude wins; on a tie the smaller row index (first maximum)
-    if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
+// |a| as an ordered 64-bit key (non-negative doubles order like their bits)
+__device__ __forceinline__ unsigned long long abs_key(double a) {
+    return (unsigned long long)__double_as_longlong(fabs(a));
 }
 
-__global__ void __launch_bounds__(kPanelThreads) k_lu_panel(double *__restrict__ M, int V, int j0, int nbc,
+// argmax over the warp of (key, row): larger key wins, smaller row on ties
+__device__ __forceinline__ void warp_argmax(unsigned long long &key, int &row) {
+    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    const bool win = (hi == mhi) && (lo == mlo);
+    const int r = (int)__reduce_min_sync(0xffffffffu, win ? (unsigned)row : 0x7fffffffu);
+    key = ((unsigned long long)mhi << 32) | mlo;
+    row = r;
+}
+
+template <int NB, int RPT>
+__global__ void __launch_bounds__(kPanelThreads) k_gj_panel(double *__restrict__ M, int V, int j0, int nbc,
                                                            int *__restrict__ ipiv, double *__restrict__ diag,
                                                            int *__restrict__ info) {
-    extern __shared__ double P[];  // [nbc][H], H = V - j0 rows j0..V-1
-    __shared__ double red_v[32];
-    __shared__ int red_i[32];
+    __shared__ double pivrow[NB], swaprow[NB];
+    __shared__ double Lt[NB][NB + 1], Ut[NB][NB + 1], Dinv[NB][NB + 1], Linv[NB][NB + 1];
+    __shared__ unsigned long long red_k[32];
+    __shared__ int red_r[32];
     __shared__ int piv_s;
-    const int H = V - j0;
-    const int tid = threadIdx.x, T = blockDim.x;
-    for (int f = tid; f < nbc * H; f += T) {
-        const int cc = f / H, r = f % H;
-        P[f] = M[(size_t)(j0 + cc) * V + j0 + r];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double a[RPT][NB];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * kPanelThreads;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) a[i][c] = (r < V && c < nbc) ? M[(size_t)(j0 + c) * V + r] : 0.0;
+    }
+#pragma unroll
+    for (int jj = 0; jj < NB; ++jj) {
+        if (jj < nbc) {
+            const int j = j0 + jj;
+            unsigned long long bk = 0;
+            int br = 0x7fffffff;
+#pragma unroll
+            for (int i = 0; i < RPT; ++i) {
+                const int r = tid + i * kPanelThreads;
+                if (r >= j && r < V) {
+                    const unsigned long long k = abs_key(a[i][jj]);
+                    if (k > bk || (k == bk && r < br)) {
+                        bk = k;
+                        br = r;
+                    }
+                }
+            }
+            warp_argmax(bk, br);
+            if (lane == 0) {
+                red_k[warp] = bk;
+                red_r[warp] = br;
+            }
+            __syncthreads();
+            if (warp == 0) {
+                bk = red_k[lane];
+                br = red_r[lane];
+                warp_argmax(bk, br);
+                if (lane == 0) {
+                    int p = br;
+                    if (bk == 0ull || p >= V) {  // exact zero column: no interchange, singular
+                        p = j;
+                        if (*info == 0) *info = j + 1;
+                    }
+                    piv_s = p;
+                    ipiv[j] = p;
+                }
+            }
+            __syncthreads();
+            const int p = piv_s;
+            // rows j and p trade places: owner of p publishes the pivot row, owner of j its own
+#pragma unroll
+            for (int i = 0; i < RPT; ++i) {
+                const int r = tid + i * kPanelThreads;
+                if (r == p) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) pivrow[c] = a[i][c];
+                }
+                if (r == j && p != j) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) swaprow[c] = a[i][c];
+                }
+            }
+            __syncthreads();
+            const double d = pivrow[jj];
+            if (tid == 0) diag[j] = d;
+            const double inv_d = 1.0 / d;
+#pragma unroll
+            for (int i = 0; i < RPT; ++i) {
+                const int r = tid + i * kPanelThreads;
+                if (r == j) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) a[i][c] = pivrow[c];
+                } else if (r == p) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) a[i][c] = swaprow[c];
+                }
+                if (r > j && r < V && d != 0.0) {
+                    const double l = a[i][jj] * inv_d;
+                    a[i][jj] = l;
+#pragma unroll
+                    for (int c = jj + 1; c < NB; ++c) a[i][c] = fma(-l, pivrow[c], a[i][c]);
+                }
+            }
+        }
+    }
+    // pivot block rows -> L11 (unit lower) and U11
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * kPanelThreads;
+        if (r >= j0 && r < j0 + nbc) {
+            const int rr = r - j0;
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                Lt[rr][c] = (c < rr) ? a[i][c] : (c == rr ? 1.0 : 0.0);
+                Ut[rr][c] = (c >= rr) ? a[i][c] : 0.0;
+            }
+        }
     }
     __syncthreads();
-    for (int jj = 0; jj < nbc; ++jj) {
-        double *col = P + (size_t)jj * H;
-        // argmax |col[r]| for r >= jj
-        double bv = -1.0;
-        int bi = 0x7fffffff;
-        for (int r = jj + tid; r < H; r += T) better(bv, bi, fabs(col[r]), r);
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_down_sync(0xffffffffu, bv, o);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            better(bv, bi, ov, oi);
+    // Linv = L11^-1 and Uinv (kept in Dinv) column by column, one thread per column
+    if (tid < nbc) {
+        const int cc = tid;
+        for (int rr = 0; rr < nbc; ++rr) {
+            double s = (rr == cc) ? 1.0 : 0.0;
+            for (int k = cc; k < rr; ++k) s = fma(-Lt[rr][k], Linv[k][cc], s);
+            Linv[rr][cc] = (rr < cc) ? 0.0 : s;
         }
-        if ((tid & 31) == 0) { red_v[tid >> 5] = bv; red_i[tid >> 5] = bi; }
-        __syncthreads();
-        if (tid < 32) {
-            bv = (tid < (T >> 5)) ? red_v[tid] : -1.0;
-            bi = (tid < (T >> 5)) ? red_i[tid] : 0x7fffffff;
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_down_sync(0xffffffffu, bv, o);
-                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-                better(bv, bi, ov, oi);
-            }
-            if (tid == 0) {
-                int p = bi;
-                if (!(bv > 0.0)) {  // exact zero column (or NaN): no interchange, record singularity
-                    p = jj;
-                    if (*info == 0) *info = j0 + jj + 1;
-                }
-                piv_s = p;
-                ipiv[j0 + jj] = j0 + p;
-            }
+        for (int rr = nbc - 1; rr >= 0; --rr) {
+            double s = (rr == cc) ? 1.0 : 0.0;
+            for (int k = rr + 1; k <= cc; ++k) s = fma(-Ut[rr][k], Dinv[k][cc], s);
+            Dinv[rr][cc] = (rr > cc) ? 0.0 : s / Ut[rr][rr];
         }
-        __syncthreads();
-        const int p = piv_s;
-        if (p != jj) {
-            for (int cc = tid; cc < nbc; cc += T) {
-                double *cl = P + (size_t)cc * H;
-                const double a = cl[jj];
-                cl[jj] = cl[p];
-                cl[p] = a;
-            }
-        }
-        __syncthreads();
-        const double d = col[jj];
-        if (tid == 0) diag[j0 + jj] = d;
-        if (d != 0.0)
-            for (int r = jj + 1 + tid; r < H; r += T) col[r] = col[r] / d;
-        __syncthreads();
-        // rank-1 update of the panel columns right of jj
-        const int w = nbc - jj - 1;
-        if (w > 0) {
-            const int rows = H - jj - 1;
-            for (int f = tid; f < w * rows; f += T) {
-                const int cc = jj + 1 + f / rows, r = jj + 1 + f % rows;
-                double *cl = P + (size_t)cc * H;
-                cl[r] = fma(-col[r], cl[jj], cl[r]);
-            }
-        }
-        __syncthreads();
     }
-    for (int f = tid; f < nbc * H; f += T) {
-        const int cc = f / H, r = f % H;
-        M[(size_t)(j0 + cc) * V + j0 + r] = P[f];
+    __syncthreads();
+    // D^-1 = Uinv Linv, written over Ut
+    if (tid < nbc * nbc) {
+        const int rr = tid / nbc, cc = tid % nbc;
+        double s = 0.0;
+        for (int k = rr; k < nbc; ++k) s = fma(Dinv[rr][k], Linv[k][cc], s);
+        Ut[rr][cc] = s;
     }
-}
-
-// Columns left of the panel: row interchanges only (LAPACK applies them to the L part too).
-__global__ void k_lu_swap_left(double *__restrict__ M, int V, int j0, int nbc, const int *__restrict__ ipiv) {
-    const int cidx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (cidx >= j0) return;
-    double *colp = M + (size_t)cidx * V;
-    for (int jj = 0; jj < nbc; ++jj) {
-        const int j = j0 + jj, p = ipiv[j];
-        if (p != j) {
-            const double a = colp[j];
-            colp[j] = colp[p];
-            colp[p] = a;
+    __syncthreads();
+    // new panel columns
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * kPanelThreads;
+        if (r >= V) continue;
+        const int kind = (r >= j0 && r < j0 + nbc) ? 0 : (r >= j0 + nbc ? 1 : 2);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            if (c >= nbc) break;
+            double s = 0.0;
+            if (kind == 0) {  // rows P: D^-1
+                s = Ut[r - j0][c];
+            } else if (kind == 1) {  // rows below: -L21 L11^-1
+#pragma unroll
+                for (int k = 0; k < NB; ++k)
+                    if (k >= c && k < nbc) s = fma(a[i][k], Linv[k][c], s);
+                s = -s;
+            } else {  // rows above the panel: -C D^-1
+#pragma unroll
+                for (int k = 0; k < NB; ++k)
+                    if (k < nbc) s = fma(a[i][k], Ut[k][c], s);
+                s = -s;
+            }
+            M[(size_t)(j0 + c) * V + r] = s;
         }
     }
 }
 
-// Trailing columns: interchanges, U12 = L11^-1 A12, A22 -= L21 U12.
-template <int CB>
-__global__ void k_lu_trail(double *__restrict__ M, int V, int j0, int nbc, const int *__restrict__ ipiv) {
-    extern __shared__ double C[];  // [CB][H]
-    const int H = V - j0;
-    const int c0 = j0 + nbc + blockIdx.x * CB;
-    const int ncol = min(CB, V - c0);
+// every column outside the panel, CB per CTA (blocks skip the panel)
+template <int NB, int CB>
+__global__ void k_gj_update(double *__restrict__ M, int V, int j0, int nbc, const int *__restrict__ ipiv) {
+    extern __shared__ double C[];  // [CB][V]
+    __shared__ double Dn[NB][NB + 1];
+    __shared__ double R[NB][CB];
+    __shared__ double Cp[NB][CB];
     const int tid = threadIdx.x, T = blockDim.x;
-    for (int f = tid; f < ncol * H; f += T) {
-        const int q = f / H, r = f % H;
-        C[f] = M[(size_t)(c0 + q) * V + j0 + r];
+    const int nleft = (j0 + CB - 1) / CB;
+    int c0, cend;
+    if ((int)blockIdx.x < nleft) {
+        c0 = blockIdx.x * CB;
+        cend = min(c0 + CB, j0);
+    } else {
+        c0 = j0 + nbc + ((int)blockIdx.x - nleft) * CB;
+        cend = min(c0 + CB, V);
     }
+    const int ncol = cend - c0;
+    if (ncol <= 0) return;
+    __shared__ int pv[NB];
+    for (int f = tid; f < ncol * V; f += T) C[f] = M[(size_t)c0 * V + f];
+    for (int f = tid; f < nbc * nbc; f += T) {
+        const int rr = f % nbc, cc = f / nbc;
+        Dn[rr][cc] = M[(size_t)(j0 + cc) * V + j0 + rr];
+    }
+    if (tid < nbc) pv[tid] = ipiv[j0 + tid];
     __syncthreads();
     if (tid < ncol) {
-        double *cl = C + (size_t)tid * H;
+        double *cl = C + (size_t)tid * V;
         for (int jj = 0; jj < nbc; ++jj) {
-            const int p = ipiv[j0 + jj] - j0;
-            if (p != jj) {
-                const double a = cl[jj];
-                cl[jj] = cl[p];
-                cl[p] = a;
+            const int j = j0 + jj, p = pv[jj];
+            if (p != j) {
+                const double t = cl[j];
+                cl[j] = cl[p];
+                cl[p] = t;
             }
         }
-        // unit lower triangular solve with L11 = A(j0+jj, j0+ii), ii < jj
-        for (int jj = 1; jj < nbc; ++jj) {
-            double acc = cl[jj];
-            for (int ii = 0; ii < jj; ++ii) acc = fma(-M[(size_t)(j0 + ii) * V + j0 + jj], cl[ii], acc);
-            cl[jj] = acc;
+    }
+    __syncthreads();
+    // pivot rows after the interchanges (A_PO) and R = D^-1 A_PO
+    for (int f = tid; f < nbc * ncol; f += T) {
+        const int jj = f % nbc, q = f / nbc;
+        Cp[jj][q] = C[(size_t)q * V + j0 + jj];
+    }
+    __syncthreads();
+    for (int f = tid; f < nbc * ncol; f += T) {
+        const int jj = f % nbc, q = f / nbc;
+        double s = 0.0;
+        for (int k = 0; k < nbc; ++k) s = fma(Dn[jj][k], Cp[k][q], s);
+        R[jj][q] = s;
+    }
+    __syncthreads();
+    // rows P: R; other rows: A - K A_PO with K = -(new panel columns)
+    for (int r = tid; r < V; r += T) {
+        if (r >= j0 && r < j0 + nbc) {
+            for (int q = 0; q < ncol; ++q) C[(size_t)q * V + r] = R[r - j0][q];
+        } else {
+            double acc[CB];
+#pragma unroll
+            for (int q = 0; q < CB; ++q) acc[q] = (q < ncol) ? C[(size_t)q * V + r] : 0.0;
+            double kr[NB];  // = -K(r, jj): all NB loads issued before the FMAs
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj) kr[jj] = (jj < nbc) ? M[(size_t)(j0 + jj) * V + r] : 0.0;
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj) {
+                if (jj < nbc) {
+#pragma unroll
+                    for (int q = 0; q < CB; ++q) acc[q] = fma(kr[jj], Cp[jj][q], acc[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < CB; ++q)
+                if (q < ncol) C[(size_t)q * V + r] = acc[q];
         }
     }
     __syncthreads();
-    // rank-nb update of rows j0+nbc .. V-1
-    for (int r = nbc + tid; r < H; r += T) {
-        double acc[CB];
-#pragma unroll
-        for (int q = 0; q < CB; ++q) acc[q] = (q < ncol) ? C[(size_t)q * H + r] : 0.0;
-        for (int jj = 0; jj < nbc; ++jj) {
-            const double l = M[(size_t)(j0 + jj) * V + j0 + r];
-#pragma unroll
-            for (int q = 0; q < CB; ++q) acc[q] = fma(-l, C[(size_t)q * H + jj], acc[q]);
-        }
-#pragma unroll
-        for (int q = 0; q < CB; ++q)
-            if (q < ncol) C[(size_t)q * H + r] = acc[q];
-    }
-    __syncthreads();
-    for (int f = tid; f < ncol * H; f += T) {
-        const int q = f / H, r = f % H;
-        M[(size_t)(c0 + q) * V + j0 + r] = C[f];
-    }
+    for (int f = tid; f < ncol * V; f += T) M[(size_t)c0 * V + f] = C[f];
 }
 
-// NR columns of A^-1 per CTA.  b = P e_c, solve L y = b (unit lower), U x = y.
-template <int NR>
-__global__ void k_lu_inverse(const double *__restrict__ LU, int V, const int *__restrict__ ipiv,
-                             double *__restrict__ X) {
-    extern __shared__ double b[];  // [V][NR]
-    __shared__ double blk[32][33];
-    __shared__ int pos_s[NR];
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int c0 = blockIdx.x * NR;
-    const int nr = min(NR, V - c0);
-    // where the single 1 of P e_c ends up after the interchanges 0..V-1
-    if (tid < nr) {
-        int pos = c0 + tid;
-        for (int j = 0; j < V; ++j) {
-            const int p = ipiv[j];
-            if (pos == j) pos = p;
-            else if (pos == p) pos = j;
-        }
-        pos_s[tid] = pos;
+// composed column permutation: applying the interchanges last-first as column
+// swaps leaves column c of the result at column src[c] of the elimination output
+__global__ void k_compose_perm(const int *__restrict__ ipiv, int V, int *__restrict__ perm) {
+    extern __shared__ int src[];  // [V] permutation, then [V] pivots
+    int *pv = src + V;
+    for (int c = threadIdx.x; c < V; c += blockDim.x) {
+        src[c] = c;
+        pv[c] = ipiv[c];
     }
     __syncthreads();
-    for (int f = tid; f < V * NR; f += T) {
-        const int r = f / NR, q = f % NR;
-        b[f] = (q < nr && r == pos_s[q]) ? 1.0 : 0.0;
+    if (threadIdx.x == 0) {
+        for (int k = V - 1; k >= 0; --k) {
+            const int p = pv[k];
+            const int t = src[k];
+            src[k] = src[p];
+            src[p] = t;
+        }
     }
     __syncthreads();
-    const int warp = tid >> 5, lane = tid & 31, nwarps = T >> 5;
-    // ---- forward: L y = b
-    for (int kb = 0; kb < V; kb += 32) {
-        const int bs = min(32, V - kb);
-        for (int f = tid; f < 32 * 32; f += T) {
-            const int rr = f % 32, kk = f / 32;  // L(kb+rr, kb+kk)
-            blk[rr][kk] = (rr < bs && kk < bs) ? LU[(size_t)(kb + kk) * V + kb + rr] : 0.0;
-        }
-        __syncthreads();
-        for (int q = warp; q < nr; q += nwarps) {
-            double val = (lane < bs) ? b[(size_t)(kb + lane) * NR + q] : 0.0;
-            for (int kk = 0; kk < bs; ++kk) {
-                const double yk = __shfl_sync(0xffffffffu, val, kk);
-                if (lane > kk) val = fma(-blk[lane][kk], yk, val);
-            }
-            if (lane < bs) b[(size_t)(kb + lane) * NR + q] = val;
-        }
-        __syncthreads();
-        for (int r = kb + bs + tid; r < V; r += T) {
-            double acc[NR];
-#pragma unroll
-            for (int q = 0; q < NR; ++q) acc[q] = b[(size_t)r * NR + q];
-            for (int kk = 0; kk < bs; ++kk) {
-                const double l = LU[(size_t)(kb + kk) * V + r];
-#pragma unroll
-                for (int q = 0; q < NR; ++q) acc[q] = fma(-l, b[(size_t)(kb + kk) * NR + q], acc[q]);
-            }
-#pragma unroll
-            for (int q = 0; q < NR; ++q) b[(size_t)r * NR + q] = acc[q];
-        }
-        __syncthreads();
-    }
-    // ---- backward: U x = y
-    for (int kend = V; kend > 0; kend -= 32) {
-        const int kb = max(0, kend - 32), bs = kend - kb;
-        for (int f = tid; f < 32 * 32; f += T) {
-            const int rr = f % 32, kk = f / 32;  // U(kb+rr, kb+kk)
-            blk[rr][kk] = (rr < bs && kk < bs) ? LU[(size_t)(kb + kk) * V + kb + rr] : 0.0;
-        }
-        __syncthreads();
-        for (int q = warp; q < nr; q += nwarps) {
-            double val = (lane < bs) ? b[(size_t)(kb + lane) * NR + q] : 0.0;
-            for (int kk = bs - 1; kk >= 0; --kk) {
-                double xk = 0.0;
-                if (lane == kk) val = val / blk[kk][kk];
-                xk = __shfl_sync(0xffffffffu, val, kk);
-                if (lane < kk) val = fma(-blk[lane][kk], xk, val);
-            }
-            if (lane < bs) b[(size_t)(kb + lane) * NR + q] = val;
-        }
-        __syncthreads();
-        for (int r = tid; r < kb; r += T) {
-            double acc[NR];
-#pragma unroll
-            for (int q = 0; q < NR; ++q) acc[q] = b[(size_t)r * NR + q];
-            for (int kk = 0; kk < bs; ++kk) {
-                const double u = LU[(size_t)(kb + kk) * V + r];
-#pragma unroll
-                for (int q = 0; q < NR; ++q) acc[q] = fma(-u, b[(size_t)(kb + kk) * NR + q], acc[q]);
-            }
-#pragma unroll
-            for (int q = 0; q < NR; ++q) b[(size_t)r * NR + q] = acc[q];
-        }
-        __syncthreads();
-    }
-    for (int f = tid; f < nr * V; f += T) {
-        const int q = f / V, r = f % V;
-        X[(size_t)(c0 + q) * V + r] = b[(size_t)r * NR + q];
-    }
+    for (int c = threadIdx.x; c < V; c += blockDim.x) perm[c] = src[c];
 }
 
-// log|det| and sign from the diagonal of U and the pivots (parallel sum).
+__global__ void k_gather_rows(const double *__restrict__ A, double *__restrict__ X, int V,
+                              const int *__restrict__ perm) {
+    const int c = blockIdx.x;
+    const int s = perm[c];
+    for (int r = threadIdx.x; r < V; r += blockDim.x) X[(size_t)c * V + r] = A[(size_t)s * V + r];
+}
+
+// log|det| and sign from U's diagonal and the pivots (parallel sum)
 __global__ void k_lu_logdet(const double *__restrict__ diag, const int *__restrict__ ipiv, int V,
                             double *__restrict__ out) {
     __shared__ double s_l[32];
@@ -293,29 +332,50 @@ __global__ void k_lu_logdet(const double *__restrict__ diag, const int *__restri
         l += __shfl_down_sync(0xffffffffu, l, o);
         neg ^= __shfl_down_sync(0xffffffffu, neg, o);
     }
-    if ((threadIdx.x & 31) == 0) { s_l[threadIdx.x >> 5] = l; s_n[threadIdx.x >> 5] = neg; }
+    if ((threadIdx.x & 31) == 0) {
+        s_l[threadIdx.x >> 5] = l;
+        s_n[threadIdx.x >> 5] = neg;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
         int n = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { t += s_l[w]; n ^= s_n[w]; }
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            t += s_l[w];
+            n ^= s_n[w];
+        }
         out[0] = t;
         out[1] = n ? -1.0 : 1.0;
     }
 }
 
-int panel_width(int V) {
-    const size_t budget = 200 * 1024 / sizeof(double);
-    int nb = 16;
-    while (nb > 1 && (size_t)nb * V > budget) nb >>= 1;
-    return nb;
+template <int NB, int RPT>
+int run_panels(double *M, LUWork &w, cudaStream_t st) {
+    const int V = w.V;
+    constexpr int CB = 8;
+    const size_t usmem = (size_t)CB * V * sizeof(double);
+    if (usmem > 200 * 1024) return EPHMC_ERR_UNSUPPORTED;
+    EPHMC_CUDA(cudaFuncSetAttribute(k_gj_update<NB, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
+    for (int j0 = 0; j0 < V; j0 += NB) {
+        const int nbc = std::min(NB, V - j0);
+        k_gj_panel<NB, RPT><<<1, kPanelThreads, 0, st>>>(M, V, j0, nbc, w.ipiv, w.diag, w.info);
+        ephmc::count_launch(1);
+        EPHMC_CUDA(cudaGetLastError());
+        const int nblocks = (j0 + CB - 1) / CB + (V - j0 - nbc + CB - 1) / CB;
+        if (nblocks > 0) {
+            k_gj_update<NB, CB><<<nblocks, 256, usmem, st>>>(M, V, j0, nbc, w.ipiv);
+            ephmc::count_launch(1);
+            EPHMC_CUDA(cudaGetLastError());
+        }
+    }
+    return EPHMC_OK;
 }
 
 }  // namespace
 
 int lu_alloc(LUWork &w, int V) {
     w.V = V;
-    EPHMC_CUDA(cudaMalloc(&w.ipiv, sizeof(int) * V));
+    EPHMC_CUDA(cudaMalloc(&w.ipiv, sizeof(int) * 2 * V));  // pivots, then the composed permutation
     EPHMC_CUDA(cudaMalloc(&w.diag, sizeof(double) * (V + 2)));
     EPHMC_CUDA(cudaMalloc(&w.info, sizeof(int) * 2));
     EPHMC_CUDA(cudaMalloc(&w.X, sizeof(double) * (size_t)V * V));
@@ -330,39 +390,25 @@ void lu_free(LUWork &w) {
     w = LUWork{};
 }
 
-int lu_factor(double *M, LUWork &w, cudaStream_t st) {
-    const int V = w.V;
-    const int nb = panel_width(V);
-    EPHMC_CUDA(cudaMemsetAsync(w.info, 0, sizeof(int) * 2, st));
-    const size_t psmem_max = (size_t)nb * V * sizeof(double);
-    EPHMC_CUDA(cudaFuncSetAttribute(k_lu_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem_max));
-    constexpr int CB = 8;
-    const size_t tsmem_max = (size_t)CB * V * sizeof(double);
-    EPHMC_CUDA(cudaFuncSetAttribute(k_lu_trail<CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem_max));
-    for (int j0 = 0; j0 < V; j0 += nb) {
-        const int nbc = std::min(nb, V - j0);
-        const int H = V - j0;
-        k_lu_panel<<<1, kPanelThreads, (size_t)nbc * H * sizeof(double), st>>>(M, V, j0, nbc, w.ipiv, w.diag, w.info); ephmc::count_launch(1);
-        EPHMC_CUDA(cudaGetLastError());
-        if (j0 > 0) {
-            k_lu_swap_left<<<(j0 + 127) / 128, 128, 0, st>>>(M, V, j0, nbc, w.ipiv); ephmc::count_launch(1);
-            EPHMC_CUDA(cudaGetLastError());
-        }
-        const int ntrail = V - j0 - nbc;
-        if (ntrail > 0) {
-            k_lu_trail<CB><<<(ntrail + CB - 1) / CB, 256, (size_t)CB * H * sizeof(double), st>>>(M, V, j0, nbc, w.ipiv); ephmc::count_launch(1);
-            EPHMC_CUDA(cudaGetLastError());
-        }
-    }
-    return EPHMC_OK;
-}
-
 int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv_host, cudaStream_t st) {
     const int V = w.V;
-    int rc = lu_factor(M, w, st);
+    EPHMC_CUDA(cudaMemsetAsync(w.info, 0, sizeof(int) * 2, st));
+    int rc;
+    if (V <= 1024) rc = run_panels<16, 1>(M, w, st);
+    else if (V <= 2048) rc = run_panels<8, 2>(M, w, st);
+    else if (V <= 4096) rc = run_panels<4, 4>(M, w, st);
+    else rc = EPHMC_ERR_UNSUPPORTED;
     if (rc != EPHMC_OK) return rc;
-    k_lu_logdet<<<1, 1024, 0, st>>>(w.diag, w.ipiv, V, w.diag + V); ephmc::count_launch(1);
+    k_lu_logdet<<<1, 1024, 0, st>>>(w.diag, w.ipiv, V, w.diag + V);
+    ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
+    int *perm = w.ipiv + V;
+    k_compose_perm<<<1, 1024, 2 * sizeof(int) * V, st>>>(w.ipiv, V, perm);
+    ephmc::count_launch(1);
+    k_gather_rows<<<V, 256, 0, st>>>(M, w.X, V, perm);
+    ephmc::count_launch(1);
+    EPHMC_CUDA(cudaGetLastError());
+    EPHMC_CUDA(cudaMemcpyAsync(M, w.X, sizeof(double) * (size_t)V * V, cudaMemcpyDeviceToDevice, st));
     int info = 0;
     double ld[2] = {0, 1};
     EPHMC_CUDA(cudaMemcpyAsync(&info, w.info, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -374,13 +420,6 @@ int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv
     if (logdet) *logdet = ld[0];
     if (sign) *sign = ld[1] < 0 ? -1 : 1;
     if (info != 0) return EPHMC_ERR_SINGULAR;
-    const size_t need = (size_t)V * V;
-    constexpr int NR = 8;
-    const size_t ismem = (size_t)V * NR * sizeof(double);
-    EPHMC_CUDA(cudaFuncSetAttribute(k_lu_inverse<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ismem));
-    k_lu_inverse<NR><<<(V + NR - 1) / NR, 256, ismem, st>>>(M, V, w.ipiv, w.X); ephmc::count_launch(1);
-    EPHMC_CUDA(cudaGetLastError());
-    EPHMC_CUDA(cudaMemcpyAsync(M, w.X, need * sizeof(double), cudaMemcpyDeviceToDevice, st));
     return EPHMC_OK;
 }
 

@@ -10,7 +10,8 @@
 //
 // Limits and sharing:
 //  * n <= kNoAllocMaxN (256): the workspace is the inverse buffer (n*n doubles),
-//    U's diagonal (n+2 doubles), the pivots (n ints) and a status flag, about
+//    U's diagonal (n+2 doubles), the pivots and their composed permutation
+//    (2n ints) and a status flag, about
 //    0.5 MB, held by every GPU that loads the library until the process exits;
 //  * all calls share that one array and it keeps the last call's contents;
 //    calls that overlap on the GPU (different streams or threads, or another
@@ -30,7 +31,7 @@ constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 constexpr size_t kOffX = 0;
 constexpr size_t kOffDiag = kOffX + align256(sizeof(double) * kNoAllocMaxN * kNoAllocMaxN);
 constexpr size_t kOffIpiv = kOffDiag + align256(sizeof(double) * (kNoAllocMaxN + 2));
-constexpr size_t kOffInfo = kOffIpiv + align256(sizeof(int) * kNoAllocMaxN);
+constexpr size_t kOffInfo = kOffIpiv + align256(sizeof(int) * 2 * kNoAllocMaxN);  // pivots + permutation
 constexpr size_t kNoAllocBytes = kOffInfo + align256(sizeof(int) * 2);
 
 // Host code must not take this symbol's address directly (that is a host-side

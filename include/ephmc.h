@@ -161,6 +161,27 @@ EPHMC_API int ephmc_ctx_create_nnt(ephmc_ctx **out, const unsigned *nnt, unsigne
                          unsigned flavors, const ephmc_flags *flags, int device);
 EPHMC_API int ephmc_ctx_set_flags(ephmc_ctx *ctx, const ephmc_flags *flags);
 
+/* force() given the inverse (simulation/organic_hmc.c:86-134): p_dot from x and
+ * M_inv (the output of logDetM_and_inv_M_hat); flags as the reference
+ * (CONSTANT_FORCE, SINGLE_PARTICLE with weight exp(-logdet), NO_FOURIER_ACC). */
+EPHMC_API int ephmc_force(ephmc_ctx *ctx, const double *x, const double *M_inv, double logdet, double *p_dot,
+                          int force_mode);
+/* construct_all_QM1P (simulation/organic_dense_matrix.c:311-381): G_t for every
+ * slice into G_out[nt*V*V]; perm_out[2*nt] (host, may be NULL) receives the
+ * slices taken on the Q side, then on the P side, as the reference's perm. */
+EPHMC_API int ephmc_all_G(ephmc_ctx *ctx, const double *x, const double *M_inv, double *G_out, int *perm_out);
+/* refine_QM1P (:383-442) of one V x V matrix in place, slice t. */
+EPHMC_API int ephmc_refine_G(ephmc_ctx *ctx, const double *x, double *G, unsigned t);
+/* apply_exp_mu_K_to_M (:209-216) on nrows rows of length V; x_slice = 3V fields. */
+EPHMC_API int ephmc_apply_exp_rows(ephmc_ctx *ctx, const double *x_slice, double *M, unsigned nrows, int revert,
+                                   int stop);
+/* out = (mu + K) in on nrows rows (apply_mu_K_to_v/_M, :96-131); add_in != 0
+ * gives out = in + (mu + K) in (apply_K_plus_1_v, :162-166). */
+EPHMC_API int ephmc_apply_stencil_rows(ephmc_ctx *ctx, const double *x_slice, const double *in, double *out,
+                                       unsigned nrows, int add_in);
+/* w = I_k v, current operator along link k (apply_current_to_v, :226-249). */
+EPHMC_API int ephmc_apply_current(ephmc_ctx *ctx, const double *x_slice, const double *v, double *w, unsigned k);
+
 /* ------------------------------------------------------------------ phonon side */
 /* Exact harmonic flow of every Matsubara mode for time h, x and p in place
  * (evolve_bosons, simulation/organic_bosons.c:126-150). */

@@ -1,0 +1,167 @@
+"""GPU tests of the drop-in surface: the reference's function names exported by
+libephmc_cuda.so, called with host pointers exactly as the reference's own C
+host code calls them, and the reference's organic_main.c linked against the
+library (oracle/_ref/organic_main_ephmc) running a whole chain."""
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ORACLE, golden, model_from_golden
+
+pytestmark = pytest.mark.gpu
+
+D, U, P, I = C.c_double, C.c_uint, C.c_void_p, C.c_int
+
+
+class OrganicFlags(C.Structure):
+    _fields_ = [("schur_form_inv", C.c_int), ("zero_filling", C.c_int), ("static_disorder", C.c_int),
+                ("single_particle", C.c_int), ("constant_force", C.c_int), ("no_fourier_acc", C.c_int),
+                ("classical_fourier_acc", C.c_int), ("cfa_steps", C.c_uint), ("cfa_mass", C.c_double)]
+
+
+def _lib():
+    import ephmc
+    lib = ephmc.load_library()
+    lib.construct_M_hat.argtypes = [P, P, P, P, P, D, P, U, U, U, P]
+    lib.construct_M_hat.restype = None
+    lib.logDetM_and_inv_M_hat.argtypes = [P, P, P, U, U, P]
+    lib.logDetM_and_inv_M_hat.restype = D
+    lib.force.argtypes = [P, P, P, P, P, P, P, P, D, D, U, P, U, U, U, D, P]
+    lib.force.restype = None
+    lib.hamilton.argtypes = [P, P, D, D, D, U, U, U, U]
+    lib.hamilton.restype = D
+    lib.apply_mu_K_to_v.argtypes = [P, P, P, P, P, D, P, U, U]
+    lib.apply_mu_K_to_v.restype = None
+    lib.apply_exp_mu_K_to_M.argtypes = [P, P, P, P, P, D, P, U, U, I, I]
+    lib.apply_exp_mu_K_to_M.restype = None
+    lib.apply_current_to_v.argtypes = [P, P, P, P, P, P, U, U, U]
+    lib.apply_current_to_v.restype = None
+    lib.construct_all_QM1P.argtypes = [P, P, P, P, P, P, P, D, P, U, U, U, P]
+    lib.construct_all_QM1P.restype = None
+    lib.ephmc_set_dropin_force_mode.argtypes = [I]
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+@pytest.mark.parametrize("name", ["small_L6_Nt64", "rect_L4x3_Nt16"])
+def test_dropin_eval_with_host_pointers(gpu, restated, name):
+    g = golden(f"eval_{name}.npz")
+    m = model_from_golden(g)
+    lib = _lib()
+    nnt = restated.lattice(m.l1, m.l2)
+    t, kap = np.array(m.t), np.array(m.kappa)
+    flags = OrganicFlags()
+    x = restated.random_x(int(g["seeds"][0]), m.dim)
+    M = np.empty(m.ns * m.ns)
+    w = np.empty(5 * m.ns * m.ns)
+    perm = np.zeros(max(m.ns, 2 * m.nt), dtype=np.int32)
+    lib.construct_M_hat(_p(x), _p(M), _p(w), _p(t), _p(kap), m.mu, _p(nnt), m.ns, 6, m.nt, C.byref(flags))
+    assert np.array_equal(M.reshape(m.ns, m.ns), g["M_hat"][0])
+    ld = lib.logDetM_and_inv_M_hat(_p(M), _p(w), _p(perm), m.ns, 1, C.byref(flags))
+    assert abs(ld - g["logdet"][0]) <= 1e-12 * abs(g["logdet"][0])
+    pd = np.empty(m.dim)
+    QM1P = np.empty(1)
+    for mode in (0, 1):
+        lib.ephmc_set_dropin_force_mode(mode)
+        lib.force(_p(x), _p(pd), _p(M), _p(QM1P), _p(w), _p(perm), _p(t), _p(kap), m.mu, m.omega, 1, _p(nnt), m.ns, 6,
+                  m.nt, ld, C.byref(flags))
+        err = np.max(np.abs(pd - g["force"][0])) / np.max(np.abs(g["force"][0]))
+        assert err <= max(1e-10, 10 * float(g["force_spread_max"][0])), (mode, err)
+    lib.ephmc_set_dropin_force_mode(0)
+    H = lib.hamilton(_p(x), None, ld, 0.0, m.omega, 1, m.ns, 6, m.nt)
+    assert abs(H - restated.hamilton(x, ld, 0.0, m.omega, 1, m.ns, m.nt)) <= 1e-12 * abs(H)
+
+
+def test_dropin_single_slice_functions(gpu, restated, reference):
+    from oracle import Model
+    m = Model.physical(4, 5, 3, 1.0)
+    lib = _lib()
+    nnt = restated.lattice(m.l1, m.l2)
+    t, kap = np.array(m.t), np.array(m.kappa)
+    x = restated.random_x(5, m.dim)
+    ctx = reference.context(m)
+    xs = x[: 3 * m.ns].copy()
+    v = restated.random_x(6, m.ns)
+    w = np.empty(m.ns)
+    lib.apply_mu_K_to_v(_p(xs), _p(v), _p(w), _p(t), _p(kap), m.mu, _p(nnt), m.ns, 6)
+    assert np.array_equal(w, ctx.apply_mu_K_v(xs, v))
+    M0 = restated.random_x(7, m.ns * m.ns)
+    for revert, stop in ((0, 2), (0, 1), (1, 0), (1, -1)):
+        Mg = M0.copy()
+        wk = np.empty(2 * m.ns * m.ns)
+        lib.apply_exp_mu_K_to_M(_p(xs), _p(Mg), _p(wk), _p(t), _p(kap), m.mu, _p(nnt), m.ns, 6, revert, stop)
+        Mr = ctx.apply_exp(xs, M0.reshape(m.ns, m.ns), revert, stop)
+        assert np.array_equal(Mg.reshape(m.ns, m.ns), Mr), (revert, stop)
+
+
+def test_dropin_all_QM1P_bit_identical(gpu, restated, reference):
+    from oracle import Model
+    m = Model.physical(4, 4, 8, 2.0)
+    lib = _lib()
+    nnt = restated.lattice(m.l1, m.l2)
+    t, kap = np.array(m.t), np.array(m.kappa)
+    x = reference.random_x(9, m.dim)
+    ctx = reference.context(m)
+    _, _, _, Mi = ctx.eval(x, want_M=True)
+    G = np.empty(m.nt * m.ns * m.ns)
+    perm = np.zeros(2 * m.nt, dtype=np.int32)
+    flags = OrganicFlags()
+    w = np.empty(5 * m.ns * m.ns)
+    lib.construct_all_QM1P(_p(x), _p(np.ascontiguousarray(Mi)), _p(G), _p(w), _p(perm), _p(t), _p(kap), m.mu,
+                           _p(nnt), m.ns, 6, m.nt, C.byref(flags))
+    assert np.array_equal(G.reshape(m.nt, m.ns, m.ns), ctx.all_QM1P(x, Mi))
+    assert np.all(perm[: m.nt] + perm[m.nt:] == m.nt - 1)
+
+
+INPUT = """4 4
+16
+4
+1 -0.5 -0.5
+0.3 0.15 0.15
+-3
+0.05
+5 0
+2
+8 1
+1 0
+0.5 0.8660254
+1
+"""
+
+
+def _read(path):
+    rows = [r for r in open(path).read().strip().split("\n") if r.strip()]
+    return np.array([[float(v) for v in r.split()] for r in rows])
+
+
+def test_reference_organic_main_linked_to_gpu_library(gpu, reference):
+    """The reference's organic_main.c + the GPU library (drop-in) against the
+    reference program on the same MT19937-64 seed: identical acceptance
+    decisions and results.csv / corr.csv rows within 1e-6."""
+    exe = os.path.join(ORACLE, "_ref", "organic_main_ephmc")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in program not built (make -C oracle dropin)")
+    with tempfile.TemporaryDirectory() as d:
+        inp = os.path.join(d, "input.txt")
+        open(inp, "w").write(INPUT)
+        r_res, r_corr = os.path.join(d, "ref_res.csv"), os.path.join(d, "ref_corr.csv")
+        g_res, g_corr = os.path.join(d, "gpu_res.csv"), os.path.join(d, "gpu_corr.csv")
+        reference.set_threads(1)
+        reference.run_main(11, inp, r_res, r_corr)
+        env = dict(os.environ, EPHMC_SEED="11")
+        out = subprocess.run([exe, inp, g_res, g_corr], env=env, capture_output=True, text=True, timeout=600)
+        assert out.returncode == 0, out.stderr
+        a, b = _read(r_res), _read(g_res)
+        assert a.shape == b.shape == (8, 12)
+        assert np.array_equal(a[:, 6], b[:, 6]), "acceptance decisions differ"
+        assert np.allclose(b, a, rtol=1e-6, atol=1e-9)
+        ca, cb = _read(r_corr), _read(g_corr)
+        assert ca.shape == cb.shape
+        assert np.allclose(cb, ca, rtol=1e-6, atol=1e-12)
