@@ -34,7 +34,7 @@ __device__ __forceinline__ Real stencil_at(const Real *__restrict__ v, int j, co
 }
 
 template <typename Real, typename QT, int S>
-__global__ void k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
+__global__ void __launch_bounds__(512) k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
                           const int *__restrict__ ev_fac, const int *__restrict__ nbr,
                           const QT *__restrict__ qstack, const double *__restrict__ Minv, int V, int nt,
                           int R, double pref_scale, double *__restrict__ force) {
@@ -189,7 +189,7 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     const int V = lat.V;
     int S = 16;
     for (int o : {1, 2, 4, 8, 16})
-        if ((V + o - 1) / o <= 256) { S = o; break; }
+        if ((V + o - 1) / o <= 512) { S = o; break; }
     const int T = (((V + S - 1) / S) + 31) / 32 * 32;
     const size_t per_vec = 9 * (size_t)V * sizeof(Real);
     const size_t fac_b = 3 * (size_t)V * sizeof(Real);

@@ -155,6 +155,9 @@ void lu_free(LUWork &w);
 // followed by the in-place inverse; log|det| and sign into host outputs.
 int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv_host,
                       cudaStream_t st);
+// Same without any host synchronisation: results stay on the device
+// (w.ipiv, w.diag[V] = log|det|, w.diag[V+1] = sign, w.info[0] = first zero pivot).
+int lu_logdet_inverse_async(double *M, LUWork &w, cudaStream_t st);
 
 // ---------------------------------------------------------------- Fourier acceleration
 // scratch: device doubles, at least fa_scratch_doubles(ld, nt)

@@ -10,19 +10,24 @@
 // of the LU factorisation: log|det| = sum log|U_ii|, the sign from the
 // diagonal signs and the pivot parity (:582-589), pivots reported 1-based.
 //
-// Per panel of nb columns p (rows P = p, others O):
-//   k_gj_panel   one 1024-thread CTA, every thread owns one row of the panel
-//                in registers: LU with partial pivoting of rows >= j0 (argmax by
-//                __reduce_max_sync on the bit pattern of |a|), then
-//                D^-1 = U11^-1 L11^-1 and the new panel columns
-//                (rows P: D^-1; rows below: -L21 L11^-1; rows above: -C D^-1);
-//   k_gj_update  every CTA owns CB other columns in shared memory: applies the
-//                panel's interchanges, sets rows P to D^-1 A(P, col) and
-//                updates the other rows A(O, col) -= K A(P, col) with
-//                K = A(O, p) D^-1 = -(new panel columns).
+// Per panel of nb columns p (rows P = pivot rows, O = all others):
+//   k_gj_panel   one CTA; every thread owns RPT rows of the panel in
+//                registers (all V rows).  Each pivot step is a full
+//                Gauss-Jordan sweep restricted to the panel columns, with one
+//                barrier: every warp publishes its best candidate row (key and
+//                values) in a double-buffered table, every warp reduces the
+//                table itself, and rows are never moved (pivoted rows are only
+//                marked; the LAPACK interchange sequence is rebuilt at the
+//                end).  After nb sweeps the panel columns hold exactly the
+//                block sweep: rows P = D^-1, rows O = -A(O,p) D^-1, written at
+//                each row's logical position.
+//   k_gj_update  every CTA owns CB other columns and a copy of the panel in
+//                shared memory: applies the panel's interchanges, sets rows P
+//                to D^-1 A(P, col) and updates the other rows
+//                A(O, col) += (new panel columns) A(P, col).
 // After the last panel the interchanges are undone as column permutations.
-// 2V^3 flops in V/nb rank-nb updates over the full matrix (GEMM-shaped, L2
-// resident at V = 1024), with no separate triangular-solve phase.
+// 2V^3 flops in V/nb rank-nb updates over the full matrix, L2 resident at
+// V = 1024, with no separate triangular-solve phase.
 #include "ephmc_internal.cuh"
 
 #include <algorithm>
@@ -32,51 +37,60 @@ namespace ephmc {
 
 namespace {
 
-constexpr int kPanelThreads = 1024;
-
 // |a| as an ordered 64-bit key (non-negative doubles order like their bits)
 __device__ __forceinline__ unsigned long long abs_key(double a) {
     return (unsigned long long)__double_as_longlong(fabs(a));
 }
 
-// argmax over the warp of (key, row): larger key wins, smaller row on ties
-__device__ __forceinline__ void warp_argmax(unsigned long long &key, int &row) {
+// argmax over the warp of (key, row): larger key wins, smaller row on ties;
+// returns the lowest lane holding the winner
+__device__ __forceinline__ int warp_argmax(unsigned long long &key, int &row) {
     const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
     const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
     const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
     const bool win = (hi == mhi) && (lo == mlo);
     const int r = (int)__reduce_min_sync(0xffffffffu, win ? (unsigned)row : 0x7fffffffu);
+    const int lane = (int)__reduce_min_sync(0xffffffffu, (win && row == r) ? (threadIdx.x & 31) : 32u);
     key = ((unsigned long long)mhi << 32) | mlo;
     row = r;
+    return lane;
 }
 
-template <int NB, int RPT>
-__global__ void __launch_bounds__(kPanelThreads) k_gj_panel(double *__restrict__ M, int V, int j0, int nbc,
-                                                           int *__restrict__ ipiv, double *__restrict__ diag,
-                                                           int *__restrict__ info) {
-    __shared__ double pivrow[NB], swaprow[NB];
-    __shared__ double Lt[NB][NB + 1], Ut[NB][NB + 1], Dinv[NB][NB + 1], Linv[NB][NB + 1];
-    __shared__ unsigned long long red_k[32];
-    __shared__ int red_r[32];
-    __shared__ int piv_s;
+template <int NB, int RPT, int T>
+__global__ void __launch_bounds__(T, 1) k_gj_panel(double *__restrict__ M, int V, int j0, int nbc,
+                                                  int *__restrict__ ipiv, double *__restrict__ diag,
+                                                  int *__restrict__ info) {
+    constexpr int NW = T / 32;
+    __shared__ unsigned long long ck[2][NW];
+    __shared__ int cr[2][NW];
+    __shared__ double crow[2][NW][NB];
+    __shared__ int chosen[NB];
+    extern __shared__ int perm_s[];  // pos[V] | where[V]
+    int *pos = perm_s, *where = perm_s + V;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double a[RPT][NB];
+    bool active[RPT];
 #pragma unroll
     for (int i = 0; i < RPT; ++i) {
-        const int r = tid + i * kPanelThreads;
+        const int r = tid + i * T;
+        active[i] = (r >= j0 && r < V);
 #pragma unroll
         for (int c = 0; c < NB; ++c) a[i][c] = (r < V && c < nbc) ? M[(size_t)(j0 + c) * V + r] : 0.0;
+    }
+    for (int r = tid; r < V; r += T) {
+        pos[r] = r;
+        where[r] = r;
     }
 #pragma unroll
     for (int jj = 0; jj < NB; ++jj) {
         if (jj < nbc) {
-            const int j = j0 + jj;
+            const int buf = jj & 1;
             unsigned long long bk = 0;
             int br = 0x7fffffff;
 #pragma unroll
             for (int i = 0; i < RPT; ++i) {
-                const int r = tid + i * kPanelThreads;
-                if (r >= j && r < V) {
+                const int r = tid + i * T;
+                if (active[i]) {
                     const unsigned long long k = abs_key(a[i][jj]);
                     if (k > bk || (k == bk && r < br)) {
                         bk = k;
@@ -85,135 +99,90 @@ __global__ void __launch_bounds__(kPanelThreads) k_gj_panel(double *__restrict__
                 }
             }
             warp_argmax(bk, br);
-            if (lane == 0) {
-                red_k[warp] = bk;
-                red_r[warp] = br;
-            }
-            __syncthreads();
-            if (warp == 0) {
-                bk = red_k[lane];
-                br = red_r[lane];
-                warp_argmax(bk, br);
-                if (lane == 0) {
-                    int p = br;
-                    if (bk == 0ull || p >= V) {  // exact zero column: no interchange, singular
-                        p = j;
-                        if (*info == 0) *info = j + 1;
-                    }
-                    piv_s = p;
-                    ipiv[j] = p;
-                }
-            }
-            __syncthreads();
-            const int p = piv_s;
-            // rows j and p trade places: owner of p publishes the pivot row, owner of j its own
 #pragma unroll
             for (int i = 0; i < RPT; ++i) {
-                const int r = tid + i * kPanelThreads;
+                if (tid + i * T == br) {
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) crow[buf][warp][c] = a[i][c];
+                }
+            }
+            if (lane == 0) {
+                ck[buf][warp] = bk;
+                cr[buf][warp] = br;
+            }
+            __syncthreads();
+            unsigned long long k = (lane < NW) ? ck[buf][lane] : 0ull;
+            int p = (lane < NW) ? cr[buf][lane] : 0x7fffffff;
+            const int w = warp_argmax(k, p);
+            const bool singular = (k == 0ull || p >= V);
+            const double *pr = crow[buf][w];
+            const double d = pr[jj];
+            const double inv_d = singular ? 0.0 : 1.0 / d;
+            if (tid == 0) {
+                chosen[jj] = singular ? -1 : p;
+                diag[j0 + jj] = singular ? 0.0 : d;
+                if (singular && *info == 0) *info = j0 + jj + 1;
+            }
+            // Gauss-Jordan sweep on the panel columns: pivot row scaled by 1/d,
+            // every other row r: a_r -= a_r[jj] * (scaled pivot row), a_r[jj] = -a_r[jj] / d
+#pragma unroll
+            for (int i = 0; i < RPT; ++i) {
+                const int r = tid + i * T;
+                if (r >= V || singular) continue;
                 if (r == p) {
 #pragma unroll
-                    for (int c = 0; c < NB; ++c) pivrow[c] = a[i][c];
-                }
-                if (r == j && p != j) {
+                    for (int c = 0; c < NB; ++c) a[i][c] = (c == jj) ? inv_d : pr[c] * inv_d;
+                    active[i] = false;
+                } else {
+                    const double f = a[i][jj];
 #pragma unroll
-                    for (int c = 0; c < NB; ++c) swaprow[c] = a[i][c];
-                }
-            }
-            __syncthreads();
-            const double d = pivrow[jj];
-            if (tid == 0) diag[j] = d;
-            const double inv_d = 1.0 / d;
-#pragma unroll
-            for (int i = 0; i < RPT; ++i) {
-                const int r = tid + i * kPanelThreads;
-                if (r == j) {
-#pragma unroll
-                    for (int c = 0; c < NB; ++c) a[i][c] = pivrow[c];
-                } else if (r == p) {
-#pragma unroll
-                    for (int c = 0; c < NB; ++c) a[i][c] = swaprow[c];
-                }
-                if (r > j && r < V && d != 0.0) {
-                    const double l = a[i][jj] * inv_d;
-                    a[i][jj] = l;
-#pragma unroll
-                    for (int c = jj + 1; c < NB; ++c) a[i][c] = fma(-l, pivrow[c], a[i][c]);
+                    for (int c = 0; c < NB; ++c)
+                        if (c != jj) a[i][c] = fma(-f, pr[c] * inv_d, a[i][c]);
+                    a[i][jj] = -f * inv_d;
                 }
             }
         }
     }
-    // pivot block rows -> L11 (unit lower) and U11
+    __syncthreads();
+    // LAPACK interchange sequence: at step j the row at logical position j
+    // trades places with the chosen row
+    if (tid == 0) {
+        for (int jj = 0; jj < nbc; ++jj) {
+            const int j = j0 + jj;
+            int pp = chosen[jj];
+            if (pp < 0) pp = pos[j];  // zero column: no interchange
+            const int q = where[pp];
+            ipiv[j] = q;
+            const int rj = pos[j];
+            pos[q] = rj;
+            where[rj] = q;
+            pos[j] = pp;
+            where[pp] = j;
+        }
+    }
+    __syncthreads();
 #pragma unroll
     for (int i = 0; i < RPT; ++i) {
-        const int r = tid + i * kPanelThreads;
-        if (r >= j0 && r < j0 + nbc) {
-            const int rr = r - j0;
-#pragma unroll
-            for (int c = 0; c < NB; ++c) {
-                Lt[rr][c] = (c < rr) ? a[i][c] : (c == rr ? 1.0 : 0.0);
-                Ut[rr][c] = (c >= rr) ? a[i][c] : 0.0;
-            }
-        }
-    }
-    __syncthreads();
-    // Linv = L11^-1 and Uinv (kept in Dinv) column by column, one thread per column
-    if (tid < nbc) {
-        const int cc = tid;
-        for (int rr = 0; rr < nbc; ++rr) {
-            double s = (rr == cc) ? 1.0 : 0.0;
-            for (int k = cc; k < rr; ++k) s = fma(-Lt[rr][k], Linv[k][cc], s);
-            Linv[rr][cc] = (rr < cc) ? 0.0 : s;
-        }
-        for (int rr = nbc - 1; rr >= 0; --rr) {
-            double s = (rr == cc) ? 1.0 : 0.0;
-            for (int k = rr + 1; k <= cc; ++k) s = fma(-Ut[rr][k], Dinv[k][cc], s);
-            Dinv[rr][cc] = (rr > cc) ? 0.0 : s / Ut[rr][rr];
-        }
-    }
-    __syncthreads();
-    // D^-1 = Uinv Linv, written over Ut
-    if (tid < nbc * nbc) {
-        const int rr = tid / nbc, cc = tid % nbc;
-        double s = 0.0;
-        for (int k = rr; k < nbc; ++k) s = fma(Dinv[rr][k], Linv[k][cc], s);
-        Ut[rr][cc] = s;
-    }
-    __syncthreads();
-    // new panel columns
-#pragma unroll
-    for (int i = 0; i < RPT; ++i) {
-        const int r = tid + i * kPanelThreads;
+        const int r = tid + i * T;
         if (r >= V) continue;
-        const int kind = (r >= j0 && r < j0 + nbc) ? 0 : (r >= j0 + nbc ? 1 : 2);
+        const int row = (r < j0) ? r : where[r];
 #pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            if (c >= nbc) break;
-            double s = 0.0;
-            if (kind == 0) {  // rows P: D^-1
-                s = Ut[r - j0][c];
-            } else if (kind == 1) {  // rows below: -L21 L11^-1
-#pragma unroll
-                for (int k = 0; k < NB; ++k)
-                    if (k >= c && k < nbc) s = fma(a[i][k], Linv[k][c], s);
-                s = -s;
-            } else {  // rows above the panel: -C D^-1
-#pragma unroll
-                for (int k = 0; k < NB; ++k)
-                    if (k < nbc) s = fma(a[i][k], Ut[k][c], s);
-                s = -s;
-            }
-            M[(size_t)(j0 + c) * V + r] = s;
-        }
+        for (int c = 0; c < NB; ++c)
+            if (c < nbc) M[(size_t)(j0 + c) * V + row] = a[i][c];
     }
 }
 
-// every column outside the panel, CB per CTA (blocks skip the panel)
+// every column outside the panel, CB per CTA (blocks skip the panel); the new
+// panel columns are staged in shared memory next to the CTA's own columns
 template <int NB, int CB>
-__global__ void k_gj_update(double *__restrict__ M, int V, int j0, int nbc, const int *__restrict__ ipiv) {
-    extern __shared__ double C[];  // [CB][V]
-    __shared__ double Dn[NB][NB + 1];
+__global__ void __launch_bounds__(256) k_gj_update(double *__restrict__ M, int V, int j0, int nbc,
+                                                   const int *__restrict__ ipiv) {
+    extern __shared__ double sm[];
+    double *C = sm;                  // [CB][V]
+    double *Pn = sm + (size_t)CB * V;  // [NB][V] new panel columns
     __shared__ double R[NB][CB];
     __shared__ double Cp[NB][CB];
+    __shared__ int pv[NB];
     const int tid = threadIdx.x, T = blockDim.x;
     const int nleft = (j0 + CB - 1) / CB;
     int c0, cend;
@@ -226,12 +195,8 @@ __global__ void k_gj_update(double *__restrict__ M, int V, int j0, int nbc, cons
     }
     const int ncol = cend - c0;
     if (ncol <= 0) return;
-    __shared__ int pv[NB];
     for (int f = tid; f < ncol * V; f += T) C[f] = M[(size_t)c0 * V + f];
-    for (int f = tid; f < nbc * nbc; f += T) {
-        const int rr = f % nbc, cc = f / nbc;
-        Dn[rr][cc] = M[(size_t)(j0 + cc) * V + j0 + rr];
-    }
+    for (int f = tid; f < nbc * V; f += T) Pn[f] = M[(size_t)j0 * V + f];
     if (tid < nbc) pv[tid] = ipiv[j0 + tid];
     __syncthreads();
     if (tid < ncol) {
@@ -246,7 +211,7 @@ __global__ void k_gj_update(double *__restrict__ M, int V, int j0, int nbc, cons
         }
     }
     __syncthreads();
-    // pivot rows after the interchanges (A_PO) and R = D^-1 A_PO
+    // pivot rows after the interchanges (A_PO) and R = D^-1 A_PO (D^-1 = rows P of the new panel)
     for (int f = tid; f < nbc * ncol; f += T) {
         const int jj = f % nbc, q = f / nbc;
         Cp[jj][q] = C[(size_t)q * V + j0 + jj];
@@ -255,32 +220,32 @@ __global__ void k_gj_update(double *__restrict__ M, int V, int j0, int nbc, cons
     for (int f = tid; f < nbc * ncol; f += T) {
         const int jj = f % nbc, q = f / nbc;
         double s = 0.0;
-        for (int k = 0; k < nbc; ++k) s = fma(Dn[jj][k], Cp[k][q], s);
+        for (int k = 0; k < nbc; ++k) s = fma(Pn[(size_t)k * V + j0 + jj], Cp[k][q], s);
         R[jj][q] = s;
     }
     __syncthreads();
-    // rows P: R; other rows: A - K A_PO with K = -(new panel columns)
+    // rows P: R; other rows: A + (new panel) A_PO.  A_PO is read from shared
+    // memory in the loop (volatile), not hoisted into NB x CB registers.
+    volatile double(*Cpv)[CB] = Cp;
     for (int r = tid; r < V; r += T) {
         if (r >= j0 && r < j0 + nbc) {
             for (int q = 0; q < ncol; ++q) C[(size_t)q * V + r] = R[r - j0][q];
-        } else {
-            double acc[CB];
-#pragma unroll
-            for (int q = 0; q < CB; ++q) acc[q] = (q < ncol) ? C[(size_t)q * V + r] : 0.0;
-            double kr[NB];  // = -K(r, jj): all NB loads issued before the FMAs
-#pragma unroll
-            for (int jj = 0; jj < NB; ++jj) kr[jj] = (jj < nbc) ? M[(size_t)(j0 + jj) * V + r] : 0.0;
-#pragma unroll
-            for (int jj = 0; jj < NB; ++jj) {
-                if (jj < nbc) {
-#pragma unroll
-                    for (int q = 0; q < CB; ++q) acc[q] = fma(kr[jj], Cp[jj][q], acc[q]);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < CB; ++q)
-                if (q < ncol) C[(size_t)q * V + r] = acc[q];
+            continue;
         }
+        double acc[CB];
+#pragma unroll
+        for (int q = 0; q < CB; ++q) acc[q] = (q < ncol) ? C[(size_t)q * V + r] : 0.0;
+#pragma unroll
+        for (int jj = 0; jj < NB; ++jj) {
+            if (jj < nbc) {
+                const double kr = Pn[(size_t)jj * V + r];
+#pragma unroll
+                for (int q = 0; q < CB; ++q) acc[q] = fma(kr, Cpv[jj][q], acc[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < CB; ++q)
+            if (q < ncol) C[(size_t)q * V + r] = acc[q];
     }
     __syncthreads();
     for (int f = tid; f < ncol * V; f += T) M[(size_t)c0 * V + f] = C[f];
@@ -349,16 +314,17 @@ __global__ void k_lu_logdet(const double *__restrict__ diag, const int *__restri
     }
 }
 
-template <int NB, int RPT>
+template <int NB, int RPT, int T, int CB>
 int run_panels(double *M, LUWork &w, cudaStream_t st) {
     const int V = w.V;
-    constexpr int CB = 8;
-    const size_t usmem = (size_t)CB * V * sizeof(double);
-    if (usmem > 200 * 1024) return EPHMC_ERR_UNSUPPORTED;
+    const size_t usmem = (size_t)(CB + NB) * V * sizeof(double);
+    const size_t psmem = 2 * (size_t)V * sizeof(int);
+    if (usmem > 210 * 1024 || psmem > 64 * 1024 || V > RPT * T) return EPHMC_ERR_UNSUPPORTED;
     EPHMC_CUDA(cudaFuncSetAttribute(k_gj_update<NB, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
+    EPHMC_CUDA(cudaFuncSetAttribute(k_gj_panel<NB, RPT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem));
     for (int j0 = 0; j0 < V; j0 += NB) {
         const int nbc = std::min(NB, V - j0);
-        k_gj_panel<NB, RPT><<<1, kPanelThreads, 0, st>>>(M, V, j0, nbc, w.ipiv, w.diag, w.info);
+        k_gj_panel<NB, RPT, T><<<1, T, psmem, st>>>(M, V, j0, nbc, w.ipiv, w.diag, w.info);
         ephmc::count_launch(1);
         EPHMC_CUDA(cudaGetLastError());
         const int nblocks = (j0 + CB - 1) / CB + (V - j0 - nbc + CB - 1) / CB;
@@ -390,13 +356,16 @@ void lu_free(LUWork &w) {
     w = LUWork{};
 }
 
-int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv_host, cudaStream_t st) {
+// Everything up to the inverse in place, asynchronous on st: pivots (0-based,
+// LAPACK order) in w.ipiv, U's diagonal in w.diag, log|det| and sign in
+// w.diag[V], w.diag[V+1], first zero pivot (1-based) in w.info[0].
+int lu_logdet_inverse_async(double *M, LUWork &w, cudaStream_t st) {
     const int V = w.V;
     EPHMC_CUDA(cudaMemsetAsync(w.info, 0, sizeof(int) * 2, st));
     int rc;
-    if (V <= 1024) rc = run_panels<16, 1>(M, w, st);
-    else if (V <= 2048) rc = run_panels<8, 2>(M, w, st);
-    else if (V <= 4096) rc = run_panels<4, 4>(M, w, st);
+    if (V <= 1024) rc = run_panels<16, 4, 256, 7>(M, w, st);
+    else if (V <= 2048) rc = run_panels<8, 4, 512, 4>(M, w, st);
+    else if (V <= 4096) rc = run_panels<4, 4, 1024, 2>(M, w, st);
     else rc = EPHMC_ERR_UNSUPPORTED;
     if (rc != EPHMC_OK) return rc;
     k_lu_logdet<<<1, 1024, 0, st>>>(w.diag, w.ipiv, V, w.diag + V);
@@ -409,6 +378,13 @@ int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv
     ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
     EPHMC_CUDA(cudaMemcpyAsync(M, w.X, sizeof(double) * (size_t)V * V, cudaMemcpyDeviceToDevice, st));
+    return EPHMC_OK;
+}
+
+int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv_host, cudaStream_t st) {
+    const int V = w.V;
+    int rc = lu_logdet_inverse_async(M, w, st);
+    if (rc != EPHMC_OK) return rc;
     int info = 0;
     double ld[2] = {0, 1};
     EPHMC_CUDA(cudaMemcpyAsync(&info, w.info, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -38,7 +38,7 @@ template <> __device__ __forceinline__ void st_as<float>(void *p, size_t i, doub
 
 // S sites per thread (site j = threadIdx.x + s*blockDim.x), R vectors per CTA.
 template <typename StackT, bool COLS, int S>
-__global__ void k_slices(const double *__restrict__ x, Couplings c,
+__global__ void __launch_bounds__(512, 2) k_slices(const double *__restrict__ x, Couplings c,
                          const int *__restrict__ ev_src, const int *__restrict__ ev_fac,
                          const SliceJob *__restrict__ jobs, int V, int R) {
     extern __shared__ double smem[];
@@ -169,7 +169,7 @@ Shape pick_shape(int V) {
     const int opts[5] = {1, 2, 4, 8, 16};
     sh.S = 16;
     for (int o : opts) {
-        if ((V + o - 1) / o <= 256) { sh.S = o; break; }
+        if ((V + o - 1) / o <= 512) { sh.S = o; break; }
     }
     const int per = (V + sh.S - 1) / sh.S;
     sh.T = ((per + 31) / 32) * 32;
