@@ -146,9 +146,12 @@ struct LUWork {
     int V = 0;
     int *ipiv = nullptr;       // device, 0-based pivot rows
     double *diag = nullptr;    // device, U_ii
-    int *info = nullptr;       // device flag
-    double *X = nullptr;       // device V*V, receives the inverse before it is copied back
+    int *info = nullptr;       // device: [0] first zero pivot (1-based), [1] dataflow wait timed out
+    double *X = nullptr;       // device V*V: panels of the dataflow kernel, or the unpermuted inverse
+    unsigned *sync = nullptr;  // device, lu_sync_words(V), zeroed once: ready flags + call counter
 };
+constexpr int kLuPanel = 8;  // columns per panel (and per CTA) of the dataflow kernel
+inline size_t lu_sync_words(int V) { return (size_t)(V + kLuPanel - 1) / kLuPanel + 1; }
 int lu_alloc(LUWork &w, int V);
 void lu_free(LUWork &w);
 // In-place LU with partial pivoting of the column-major matrix A(r,c) = M[c*V+r],

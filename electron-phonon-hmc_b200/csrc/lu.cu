@@ -251,6 +251,290 @@ __global__ void __launch_bounds__(256) k_gj_update(double *__restrict__ M, int V
     for (int f = tid; f < ncol * V; f += T) M[(size_t)c0 * V + f] = C[f];
 }
 
+// ---------------------------------------------------------------- dataflow kernel
+// One cooperative launch for the whole factorisation and inverse (V <= 1024).
+// CTA b owns columns [8b, 8b+8) of A for the entire run, one row per thread,
+// in registers.  Panels are processed in order; panel k is CTA k's own block:
+//   * CTA k, once its block has received panels 0..k-1, runs the 8 pivot
+//     steps on it (Gauss-Jordan sweep restricted to the block) and publishes
+//     the swept block, the pivots and U's diagonal, then a ready flag;
+//   * every other CTA waits for that flag and applies the block update to its
+//     own columns: with K = published block and A_P = its rows at the 8 pivot
+//     positions, rows P become K_P A_P and all other rows r add K_r A_P.
+// Rows never move.  Each thread tracks the logical position (LAPACK's row
+// order after interchanges) of its row by replaying the interchanges, which
+// also gives the dgetrf tie-break (first logical row among equal magnitudes)
+// and the final placement: the inverse is X(lpos(r), P_j) = Y(r, j), with P_j
+// the physical pivot row of step j and Y the array after the last panel.
+// The ready flags (ready[0..nblk)) carry a per-call epoch, one more than the
+// call counter ready[nblk] that every CTA reads at its start and the last
+// panel's owner advances at its end, so they are never reset and a captured
+// launch can be replayed.  Waits are bounded (kLuWaitNs): on expiry the CTA
+// sets info[1] and leaves.
+constexpr unsigned long long kLuWaitNs = 2000000000ull;
+constexpr unsigned kLuWaitPolls = 1u << 26;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// true once *f == epoch; false when the wait runs out (time or poll count).
+// sleep_ns > 0 spaces the polls of waiters that are not on the critical path.
+__device__ bool wait_ready(const unsigned *f, unsigned epoch, unsigned sleep_ns) {
+    if (ld_acquire_u32(f) == epoch) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned n = 0; n < kLuWaitPolls; ++n) {
+        if (sleep_ns) __nanosleep(sleep_ns);
+        if (ld_acquire_u32(f) == epoch) return true;
+        if (global_ns() - t0 > kLuWaitNs) break;
+    }
+    return false;
+}
+
+// argmax of (key, lp) over the 32 lanes: larger key, then smaller logical
+// position.  Returns true in the one lane holding the winner (logical
+// positions are distinct); when no lane has a candidate (lp == INT_MAX
+// everywhere) lane 0 is the winner.
+__device__ __forceinline__ bool warp_argmax_lpos(unsigned long long &key, int &lp) {
+    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    const bool win = (hi == mhi) && (lo == mlo);
+    const int ml = (int)__reduce_min_sync(0xffffffffu, win ? (unsigned)lp : 0x7fffffffu);
+    const bool me = win && lp == ml && (ml != 0x7fffffff || (threadIdx.x & 31) == 0);
+    key = ((unsigned long long)mhi << 32) | mlo;
+    lp = ml;
+    return me;
+}
+
+// Same result as warp_argmax_lpos, with a shortcut for the usual case of a
+// unique largest high word (sign, exponent and 20 mantissa bits of |value|):
+// then that lane wins without comparing low words or positions.  Unlike
+// warp_argmax_lpos it leaves key and lp as they were in every lane.
+__device__ __forceinline__ bool warp_argmax_fast(unsigned long long &key, int &lp) {
+    const unsigned hi = (unsigned)(key >> 32);
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned tied = __ballot_sync(0xffffffffu, hi == mhi);
+    if (mhi != 0u && __popc(tied) == 1) return hi == mhi;
+    unsigned long long k2 = key;
+    int l2 = lp;
+    return warp_argmax_lpos(k2, l2);
+}
+
+// 1/d by two Newton-Raphson steps x <- x + x (1 - d x) from the hardware
+// reciprocal approximation (PTX rcp.approx.ftz.f64); within one unit in the
+// last place of the correctly rounded quotient for normal d.
+__device__ __forceinline__ double recip_nr(double d) {
+    double x;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(d));
+    double e = fma(-d, x, 1.0);
+    x = fma(x, e, x);
+    e = fma(-d, x, 1.0);
+    return fma(x, e, x);
+}
+
+template <int NB>
+__device__ __forceinline__ void rotate_left(double (&a)[NB]) {
+    const double t = a[0];
+#pragma unroll
+    for (int q = 0; q + 1 < NB; ++q) a[q] = a[q + 1];
+    a[NB - 1] = t;
+}
+
+template <int NB>
+__global__ void __launch_bounds__(1024, 1) k_gj_dataflow(double *__restrict__ M, int V,
+                                                         double *__restrict__ panels, int *__restrict__ ipiv,
+                                                         double *__restrict__ diag, int *__restrict__ info,
+                                                         unsigned *__restrict__ ready) {
+    constexpr int MW = 32;
+    // per warp candidate of a pivot step: |value| key, logical position,
+    // physical row, and the row already divided by its own pivot entry
+    __shared__ unsigned long long ck[2][MW];
+    __shared__ int cl[2][MW], cphys[2][MW];
+    __shared__ double cval[2][MW];
+    __shared__ __align__(16) double crow[2][MW][NB];
+    __shared__ double Cp[2][NB][NB];
+    __shared__ int s_ip[2][NB];
+    __shared__ int own_p[NB];
+    __shared__ int s_abort;
+    __shared__ unsigned s_epoch;
+    __shared__ double s_l[MW];
+    __shared__ int s_n[MW];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = (int)(blockDim.x >> 5);
+    const int b = blockIdx.x, nblk = gridDim.x;
+    const int c0 = b * NB, ncol = min(NB, V - c0);
+    const int r = tid;
+    const bool valid = r < V;
+    int lpos = r;
+    double a[NB];
+#pragma unroll
+    for (int q = 0; q < NB; ++q) a[q] = (valid && q < ncol) ? M[(size_t)(c0 + q) * V + r] : 0.0;
+    if (tid == 0) {
+        s_abort = 0;
+        const unsigned e = __ldcg(ready + nblk) + 1u;
+        s_epoch = e ? e : 1u;
+    }
+    __syncthreads();
+    const unsigned epoch = s_epoch;
+
+    for (int k = 0; k < nblk; ++k) {
+        const int j0 = k * NB, nbc = min(NB, V - j0);
+        if (k == b) {
+            // the block is rotated one column left after every step, so the
+            // pivot column is always a[0]; nbc + (NB - nbc) rotations restore it
+            for (int jj = 0; jj < nbc; ++jj) {
+                const int j = j0 + jj, buf = jj & 1;
+                const double a0 = a[0];
+                unsigned long long key = 0ull;
+                int lp = 0x7fffffff;
+                if (valid && lpos >= j) {
+                    key = (unsigned long long)__double_as_longlong(fabs(a0));
+                    lp = lpos;
+                }
+                if (warp_argmax_fast(key, lp)) {
+                    const double inv = (key == 0ull) ? 0.0 : recip_nr(a0);
+                    ck[buf][warp] = key;
+                    cl[buf][warp] = lp;
+                    cphys[buf][warp] = r;
+                    cval[buf][warp] = a0;
+                    crow[buf][warp][0] = inv;
+#pragma unroll
+                    for (int q = 1; q < NB; ++q) crow[buf][warp][q] = a[q] * inv;
+                }
+                __syncthreads();
+                unsigned long long kb = (lane < NW) ? ck[buf][lane] : 0ull;
+                int lb = (lane < NW) ? cl[buf][lane] : 0x7fffffff;
+                const bool wme = warp_argmax_fast(kb, lb) && lane < NW;
+                const int w = __ffs(__ballot_sync(0xffffffffu, wme)) - 1;
+                const int p = cphys[buf][w];
+                lb = cl[buf][w];
+                double prs[NB];
+#pragma unroll
+                for (int q = 0; q < NB; q += 2) {
+                    const double2 t2 = *reinterpret_cast<const double2 *>(&crow[buf][w][q]);
+                    prs[q] = t2.x;
+                    prs[q + 1] = t2.y;
+                }
+                if (tid == 0) {
+                    const bool singular = (ck[buf][w] == 0ull);
+                    ipiv[j] = lb;
+                    diag[j] = singular ? 0.0 : cval[buf][w];
+                    own_p[jj] = p;
+                    if (singular) atomicCAS(info, 0, j + 1);
+                }
+                if (r == p) {
+#pragma unroll
+                    for (int q = 0; q < NB; ++q) a[q] = prs[q];
+                } else {
+                    a[0] = -a0 * prs[0];
+#pragma unroll
+                    for (int q = 1; q < NB; ++q) a[q] = fma(-a0, prs[q], a[q]);
+                }
+                if (lpos == j) lpos = lb;
+                else if (lpos == lb) lpos = j;
+                rotate_left(a);
+            }
+            for (int e = nbc; e < NB; ++e) rotate_left(a);
+#pragma unroll
+            for (int q = 0; q < NB; ++q)
+                if (valid && q < nbc) panels[(size_t)(j0 + q) * V + r] = a[q];
+            __syncthreads();
+            if (tid == 0) st_release_u32(ready + k, epoch);
+        } else {
+            const int buf = k & 1;
+            // one warp waits and fetches the panel's pivots; the next owner
+            // polls without pause, the others space their polls
+            if (warp == 0) {
+                int ok = 1;
+                if (lane == 0) ok = wait_ready(ready + k, epoch, b == k + 1 ? 0u : 256u);
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                __syncwarp();
+                if (ok) {
+                    if (lane < nbc) s_ip[buf][lane] = __ldcg(ipiv + j0 + lane);
+                } else if (lane == 0) {
+                    s_abort = 1;
+                    atomicExch(info + 1, 1);
+                }
+            }
+            __syncthreads();
+            if (s_abort) return;
+            double kv[NB];
+#pragma unroll
+            for (int m = 0; m < NB; ++m) kv[m] = (valid && m < nbc) ? __ldcg(panels + (size_t)(j0 + m) * V + r) : 0.0;
+#pragma unroll
+            for (int m = 0; m < NB; ++m) {
+                if (m < nbc) {
+                    const int j = j0 + m, ip = s_ip[buf][m];
+                    if (lpos == j) lpos = ip;
+                    else if (lpos == ip) lpos = j;
+                }
+            }
+            const bool is_p = valid && lpos >= j0 && lpos < j0 + nbc;
+            if (is_p) {
+#pragma unroll
+                for (int q = 0; q < NB; ++q) Cp[buf][lpos - j0][q] = a[q];
+            }
+            __syncthreads();
+            if (valid) {
+#pragma unroll
+                for (int q = 0; q < NB; ++q) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int m = 0; m < NB; ++m)
+                        if (m < nbc) s = fma(kv[m], Cp[buf][m][q], s);
+                    a[q] = is_p ? s : a[q] + s;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // every panel has been seen: place the inverse, X(lpos, P_j) = Y(r, j)
+#pragma unroll
+    for (int q = 0; q < NB; ++q)
+        if (valid && q < ncol) M[(size_t)own_p[q] * V + lpos] = a[q];
+    // the last panel's owner has acquired every flag: log|det| and sign
+    if (b == nblk - 1) {
+        double l = 0.0;
+        int neg = 0;
+        for (int i = tid; i < V; i += blockDim.x) {
+            const double d = __ldcg(diag + i);
+            l += log(fabs(d));
+            if (!(d > 0)) neg ^= 1;
+            if (__ldcg(ipiv + i) != i) neg ^= 1;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            l += __shfl_down_sync(0xffffffffu, l, o);
+            neg ^= __shfl_down_sync(0xffffffffu, neg, o);
+        }
+        if (lane == 0) {
+            s_l[warp] = l;
+            s_n[warp] = neg;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            int n = 0;
+            for (int i = 0; i < NW; ++i) {
+                t += s_l[i];
+                n ^= s_n[i];
+            }
+            diag[V] = t;
+            diag[V + 1] = n ? -1.0 : 1.0;
+            ready[nblk] = epoch;
+        }
+    }
+}
+
 // composed column permutation: applying the interchanges last-first as column
 // swaps leaves column c of the result at column src[c] of the elimination output
 __global__ void k_compose_perm(const int *__restrict__ ipiv, int V, int *__restrict__ perm) {
@@ -337,6 +621,26 @@ int run_panels(double *M, LUWork &w, cudaStream_t st) {
     return EPHMC_OK;
 }
 
+// The dataflow kernel needs all ceil(V/8) CTAs resident at once; returns
+// EPHMC_ERR_UNSUPPORTED (nothing launched) when they are not, or V > 1024.
+int run_dataflow(double *M, LUWork &w, cudaStream_t st) {
+    const int V = w.V;
+    if (V > 1024 || w.sync == nullptr) return EPHMC_ERR_UNSUPPORTED;
+    const int nblk = (V + kLuPanel - 1) / kLuPanel;
+    const int T = (V + 31) / 32 * 32;
+    int dev = 0, sms = 0, coop = 0, per_sm = 0;
+    EPHMC_CUDA(cudaGetDevice(&dev));
+    EPHMC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    EPHMC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    EPHMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_dataflow<kLuPanel>, T, 0));
+    if (!coop || (long)per_sm * sms < nblk) return EPHMC_ERR_UNSUPPORTED;
+    double *panels = w.X;
+    void *args[] = {&M, (void *)&V, &panels, &w.ipiv, &w.diag, &w.info, &w.sync};
+    EPHMC_CUDA(cudaLaunchCooperativeKernel((const void *)k_gj_dataflow<kLuPanel>, dim3(nblk), dim3(T), args, 0, st));
+    ephmc::count_launch(1);
+    return EPHMC_OK;
+}
+
 }  // namespace
 
 int lu_alloc(LUWork &w, int V) {
@@ -345,6 +649,8 @@ int lu_alloc(LUWork &w, int V) {
     EPHMC_CUDA(cudaMalloc(&w.diag, sizeof(double) * (V + 2)));
     EPHMC_CUDA(cudaMalloc(&w.info, sizeof(int) * 2));
     EPHMC_CUDA(cudaMalloc(&w.X, sizeof(double) * (size_t)V * V));
+    EPHMC_CUDA(cudaMalloc(&w.sync, sizeof(unsigned) * lu_sync_words(V)));
+    EPHMC_CUDA(cudaMemset(w.sync, 0, sizeof(unsigned) * lu_sync_words(V)));
     return EPHMC_OK;
 }
 
@@ -353,6 +659,7 @@ void lu_free(LUWork &w) {
     if (w.diag) cudaFree(w.diag);
     if (w.info) cudaFree(w.info);
     if (w.X) cudaFree(w.X);
+    if (w.sync) cudaFree(w.sync);
     w = LUWork{};
 }
 
@@ -362,7 +669,9 @@ void lu_free(LUWork &w) {
 int lu_logdet_inverse_async(double *M, LUWork &w, cudaStream_t st) {
     const int V = w.V;
     EPHMC_CUDA(cudaMemsetAsync(w.info, 0, sizeof(int) * 2, st));
-    int rc;
+    int rc = run_dataflow(M, w, st);
+    if (rc == EPHMC_OK) return EPHMC_OK;
+    if (rc != EPHMC_ERR_UNSUPPORTED) return rc;
     if (V <= 1024) rc = run_panels<16, 4, 256, 7>(M, w, st);
     else if (V <= 2048) rc = run_panels<8, 4, 512, 4>(M, w, st);
     else if (V <= 4096) rc = run_panels<4, 4, 1024, 2>(M, w, st);
@@ -385,9 +694,9 @@ int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv
     const int V = w.V;
     int rc = lu_logdet_inverse_async(M, w, st);
     if (rc != EPHMC_OK) return rc;
-    int info = 0;
+    int info[2] = {0, 0};
     double ld[2] = {0, 1};
-    EPHMC_CUDA(cudaMemcpyAsync(&info, w.info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EPHMC_CUDA(cudaMemcpyAsync(info, w.info, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
     EPHMC_CUDA(cudaMemcpyAsync(ld, w.diag + V, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
     if (ipiv_host) EPHMC_CUDA(cudaMemcpyAsync(ipiv_host, w.ipiv, sizeof(int) * V, cudaMemcpyDeviceToHost, st));
     EPHMC_CUDA(cudaStreamSynchronize(st));
@@ -395,7 +704,14 @@ int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv
         for (int i = 0; i < V; ++i) ipiv_host[i] += 1;  // LAPACK 1-based
     if (logdet) *logdet = ld[0];
     if (sign) *sign = ld[1] < 0 ? -1 : 1;
-    if (info != 0) return EPHMC_ERR_SINGULAR;
+    if (info[1] != 0) {
+        // flags of the abandoned call could match the next call's epoch
+        cudaMemsetAsync(w.sync, 0, sizeof(unsigned) * lu_sync_words(V), st);
+        cudaStreamSynchronize(st);
+        set_status(EPHMC_ERR_TIMEOUT, "LU: a panel wait of the dataflow kernel ran out; the result is invalid");
+        return EPHMC_ERR_TIMEOUT;
+    }
+    if (info[0] != 0) return EPHMC_ERR_SINGULAR;
     return EPHMC_OK;
 }
 

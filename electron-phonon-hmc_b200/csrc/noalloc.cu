@@ -11,7 +11,7 @@
 // Limits and sharing:
 //  * n <= kNoAllocMaxN (256): the workspace is the inverse buffer (n*n doubles),
 //    U's diagonal (n+2 doubles), the pivots and their composed permutation
-//    (2n ints) and a status flag, about
+//    (2n ints), status flags and the LU kernel's panel flags, about
 //    0.5 MB, held by every GPU that loads the library until the process exits;
 //  * all calls share that one array and it keeps the last call's contents;
 //    calls that overlap on the GPU (different streams or threads, or another
@@ -32,7 +32,8 @@ constexpr size_t kOffX = 0;
 constexpr size_t kOffDiag = kOffX + align256(sizeof(double) * kNoAllocMaxN * kNoAllocMaxN);
 constexpr size_t kOffIpiv = kOffDiag + align256(sizeof(double) * (kNoAllocMaxN + 2));
 constexpr size_t kOffInfo = kOffIpiv + align256(sizeof(int) * 2 * kNoAllocMaxN);  // pivots + permutation
-constexpr size_t kNoAllocBytes = kOffInfo + align256(sizeof(int) * 2);
+constexpr size_t kOffSync = kOffInfo + align256(sizeof(int) * 2);
+constexpr size_t kNoAllocBytes = kOffSync + align256(sizeof(unsigned) * ((kNoAllocMaxN + ephmc::kLuPanel - 1) / ephmc::kLuPanel + 1));
 
 // Host code must not take this symbol's address directly (that is a host-side
 // stand-in); the device address comes from cudaGetSymbolAddress below.
@@ -92,6 +93,7 @@ EPHMC_API int ephmc_logdet_inverse_noalloc(double *M, unsigned n, double *logdet
     w.diag = reinterpret_cast<double *>(base + kOffDiag);
     w.ipiv = reinterpret_cast<int *>(base + kOffIpiv);
     w.info = reinterpret_cast<int *>(base + kOffInfo);  // zeroed by the factorisation itself
+    w.sync = reinterpret_cast<unsigned *>(base + kOffSync);  // zero-initialised with the module
     int sg = 1;
     double ld = 0;
     rc = ephmc::lu_logdet_inverse(M, w, &ld, &sg, ipiv, static_cast<cudaStream_t>(stream));
