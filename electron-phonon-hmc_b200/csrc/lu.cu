@@ -350,19 +350,20 @@ __device__ __forceinline__ void rotate_left(double (&a)[NB]) {
     a[NB - 1] = t;
 }
 
-template <int NB>
-__global__ void __launch_bounds__(1024, 1) k_gj_dataflow(double *__restrict__ M, int V,
-                                                         double *__restrict__ panels, int *__restrict__ ipiv,
-                                                         double *__restrict__ diag, int *__restrict__ info,
-                                                         unsigned *__restrict__ ready) {
-    constexpr int MW = 32;
+// RPT rows per thread (rows tid, tid + T, ...), T = blockDim.x <= 256.
+template <int NB, int RPT>
+__global__ void __launch_bounds__(256, 1) k_gj_dataflow(double *__restrict__ M, int V,
+                                                        double *__restrict__ panels, int *__restrict__ ipiv,
+                                                        double *__restrict__ diag, int *__restrict__ info,
+                                                        unsigned *__restrict__ ready) {
+    constexpr int MW = 8;
     // per warp candidate of a pivot step: |value| key, logical position,
-    // physical row, and the row already divided by its own pivot entry
+    // physical row, value, and the row already divided by its pivot entry
     __shared__ unsigned long long ck[2][MW];
     __shared__ int cl[2][MW], cphys[2][MW];
     __shared__ double cval[2][MW];
     __shared__ __align__(16) double crow[2][MW][NB];
-    __shared__ double Cp[2][NB][NB];
+    __shared__ __align__(16) double Cp[2][NB][NB];
     __shared__ int s_ip[2][NB];
     __shared__ int own_p[NB];
     __shared__ int s_abort;
@@ -370,15 +371,18 @@ __global__ void __launch_bounds__(1024, 1) k_gj_dataflow(double *__restrict__ M,
     __shared__ double s_l[MW];
     __shared__ int s_n[MW];
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, NW = (int)(blockDim.x >> 5);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, T = (int)blockDim.x, NW = T >> 5;
     const int b = blockIdx.x, nblk = gridDim.x;
     const int c0 = b * NB, ncol = min(NB, V - c0);
-    const int r = tid;
-    const bool valid = r < V;
-    int lpos = r;
-    double a[NB];
+    int row[RPT], lpos[RPT];
+    double a[RPT][NB];
 #pragma unroll
-    for (int q = 0; q < NB; ++q) a[q] = (valid && q < ncol) ? M[(size_t)(c0 + q) * V + r] : 0.0;
+    for (int i = 0; i < RPT; ++i) {
+        row[i] = tid + i * T;
+        lpos[i] = row[i];
+#pragma unroll
+        for (int q = 0; q < NB; ++q) a[i][q] = (row[i] < V && q < ncol) ? M[(size_t)(c0 + q) * V + row[i]] : 0.0;
+    }
     if (tid == 0) {
         s_abort = 0;
         const unsigned e = __ldcg(ready + nblk) + 1u;
@@ -391,25 +395,40 @@ __global__ void __launch_bounds__(1024, 1) k_gj_dataflow(double *__restrict__ M,
         const int j0 = k * NB, nbc = min(NB, V - j0);
         if (k == b) {
             // the block is rotated one column left after every step, so the
-            // pivot column is always a[0]; nbc + (NB - nbc) rotations restore it
+            // pivot column is always a[.][0]; NB rotations in all restore it
             for (int jj = 0; jj < nbc; ++jj) {
                 const int j = j0 + jj, buf = jj & 1;
-                const double a0 = a[0];
                 unsigned long long key = 0ull;
-                int lp = 0x7fffffff;
-                if (valid && lpos >= j) {
-                    key = (unsigned long long)__double_as_longlong(fabs(a0));
-                    lp = lpos;
+                int lp = 0x7fffffff, bi = 0;
+#pragma unroll
+                for (int i = 0; i < RPT; ++i) {
+                    if (row[i] < V && lpos[i] >= j) {
+                        const unsigned long long ki = (unsigned long long)__double_as_longlong(fabs(a[i][0]));
+                        if (ki > key || (ki == key && lpos[i] < lp)) {
+                            key = ki;
+                            lp = lpos[i];
+                            bi = i;
+                        }
+                    }
                 }
                 if (warp_argmax_fast(key, lp)) {
-                    const double inv = (key == 0ull) ? 0.0 : recip_nr(a0);
+                    double v[NB];
+#pragma unroll
+                    for (int q = 0; q < NB; ++q) v[q] = a[0][q];
+#pragma unroll
+                    for (int i = 1; i < RPT; ++i)
+                        if (bi == i) {
+#pragma unroll
+                            for (int q = 0; q < NB; ++q) v[q] = a[i][q];
+                        }
+                    const double inv = (key == 0ull) ? 0.0 : recip_nr(v[0]);
                     ck[buf][warp] = key;
                     cl[buf][warp] = lp;
-                    cphys[buf][warp] = r;
-                    cval[buf][warp] = a0;
+                    cphys[buf][warp] = row[bi];
+                    cval[buf][warp] = v[0];
                     crow[buf][warp][0] = inv;
 #pragma unroll
-                    for (int q = 1; q < NB; ++q) crow[buf][warp][q] = a[q] * inv;
+                    for (int q = 1; q < NB; ++q) crow[buf][warp][q] = v[q] * inv;
                 }
                 __syncthreads();
                 unsigned long long kb = (lane < NW) ? ck[buf][lane] : 0ull;
@@ -432,22 +451,31 @@ __global__ void __launch_bounds__(1024, 1) k_gj_dataflow(double *__restrict__ M,
                     own_p[jj] = p;
                     if (singular) atomicCAS(info, 0, j + 1);
                 }
-                if (r == p) {
 #pragma unroll
-                    for (int q = 0; q < NB; ++q) a[q] = prs[q];
-                } else {
-                    a[0] = -a0 * prs[0];
+                for (int i = 0; i < RPT; ++i) {
+                    if (row[i] == p) {
 #pragma unroll
-                    for (int q = 1; q < NB; ++q) a[q] = fma(-a0, prs[q], a[q]);
+                        for (int q = 0; q < NB; ++q) a[i][q] = prs[q];
+                    } else {
+                        const double f = a[i][0];
+                        a[i][0] = -f * prs[0];
+#pragma unroll
+                        for (int q = 1; q < NB; ++q) a[i][q] = fma(-f, prs[q], a[i][q]);
+                    }
+                    if (lpos[i] == j) lpos[i] = lb;
+                    else if (lpos[i] == lb) lpos[i] = j;
+                    rotate_left(a[i]);
                 }
-                if (lpos == j) lpos = lb;
-                else if (lpos == lb) lpos = j;
-                rotate_left(a);
             }
-            for (int e = nbc; e < NB; ++e) rotate_left(a);
+            for (int e = nbc; e < NB; ++e) {
 #pragma unroll
-            for (int q = 0; q < NB; ++q)
-                if (valid && q < nbc) panels[(size_t)(j0 + q) * V + r] = a[q];
+                for (int i = 0; i < RPT; ++i) rotate_left(a[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < RPT; ++i)
+#pragma unroll
+                for (int q = 0; q < NB; ++q)
+                    if (row[i] < V && q < nbc) panels[(size_t)(j0 + q) * V + row[i]] = a[i][q];
             __syncthreads();
             if (tid == 0) st_release_u32(ready + k, epoch);
         } else {
@@ -468,31 +496,41 @@ __global__ void __launch_bounds__(1024, 1) k_gj_dataflow(double *__restrict__ M,
             }
             __syncthreads();
             if (s_abort) return;
-            double kv[NB];
+            double kv[RPT][NB];
 #pragma unroll
-            for (int m = 0; m < NB; ++m) kv[m] = (valid && m < nbc) ? __ldcg(panels + (size_t)(j0 + m) * V + r) : 0.0;
+            for (int i = 0; i < RPT; ++i)
 #pragma unroll
-            for (int m = 0; m < NB; ++m) {
-                if (m < nbc) {
-                    const int j = j0 + m, ip = s_ip[buf][m];
-                    if (lpos == j) lpos = ip;
-                    else if (lpos == ip) lpos = j;
+                for (int m = 0; m < NB; ++m)
+                    kv[i][m] = (row[i] < V && m < nbc) ? __ldcg(panels + (size_t)(j0 + m) * V + row[i]) : 0.0;
+            bool is_p[RPT];
+#pragma unroll
+            for (int i = 0; i < RPT; ++i) {
+#pragma unroll
+                for (int m = 0; m < NB; ++m) {
+                    if (m < nbc) {
+                        const int j = j0 + m, ip = s_ip[buf][m];
+                        if (lpos[i] == j) lpos[i] = ip;
+                        else if (lpos[i] == ip) lpos[i] = j;
+                    }
+                }
+                is_p[i] = row[i] < V && lpos[i] >= j0 && lpos[i] < j0 + nbc;
+                if (is_p[i]) {
+#pragma unroll
+                    for (int q = 0; q < NB; ++q) Cp[buf][lpos[i] - j0][q] = a[i][q];
                 }
             }
-            const bool is_p = valid && lpos >= j0 && lpos < j0 + nbc;
-            if (is_p) {
-#pragma unroll
-                for (int q = 0; q < NB; ++q) Cp[buf][lpos - j0][q] = a[q];
-            }
             __syncthreads();
-            if (valid) {
 #pragma unroll
-                for (int q = 0; q < NB; ++q) {
+            for (int q = 0; q < NB; ++q) {
+                double cp[NB];
+#pragma unroll
+                for (int m = 0; m < NB; ++m) cp[m] = (m < nbc) ? Cp[buf][m][q] : 0.0;
+#pragma unroll
+                for (int i = 0; i < RPT; ++i) {
                     double s = 0.0;
 #pragma unroll
-                    for (int m = 0; m < NB; ++m)
-                        if (m < nbc) s = fma(kv[m], Cp[buf][m][q], s);
-                    a[q] = is_p ? s : a[q] + s;
+                    for (int m = 0; m < NB; ++m) s = fma(kv[i][m], cp[m], s);
+                    a[i][q] = is_p[i] ? s : a[i][q] + s;
                 }
             }
         }
@@ -500,13 +538,15 @@ __global__ void __launch_bounds__(1024, 1) k_gj_dataflow(double *__restrict__ M,
     __syncthreads();
     // every panel has been seen: place the inverse, X(lpos, P_j) = Y(r, j)
 #pragma unroll
-    for (int q = 0; q < NB; ++q)
-        if (valid && q < ncol) M[(size_t)own_p[q] * V + lpos] = a[q];
+    for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int q = 0; q < NB; ++q)
+            if (row[i] < V && q < ncol) M[(size_t)own_p[q] * V + lpos[i]] = a[i][q];
     // the last panel's owner has acquired every flag: log|det| and sign
     if (b == nblk - 1) {
         double l = 0.0;
         int neg = 0;
-        for (int i = tid; i < V; i += blockDim.x) {
+        for (int i = tid; i < V; i += T) {
             const double d = __ldcg(diag + i);
             l += log(fabs(d));
             if (!(d > 0)) neg ^= 1;
@@ -621,24 +661,37 @@ int run_panels(double *M, LUWork &w, cudaStream_t st) {
     return EPHMC_OK;
 }
 
+template <int RPT>
+int launch_dataflow(double *M, LUWork &w, int nblk, int T, int sms, cudaStream_t st) {
+    int per_sm = 0;
+    EPHMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_dataflow<kLuPanel, RPT>, T, 0));
+    if ((long)per_sm * sms < nblk) return EPHMC_ERR_UNSUPPORTED;
+    const int V = w.V;
+    double *panels = w.X;
+    void *args[] = {&M, (void *)&V, &panels, &w.ipiv, &w.diag, &w.info, &w.sync};
+    EPHMC_CUDA(cudaLaunchCooperativeKernel((const void *)k_gj_dataflow<kLuPanel, RPT>, dim3(nblk), dim3(T), args, 0,
+                                           st));
+    ephmc::count_launch(1);
+    return EPHMC_OK;
+}
+
 // The dataflow kernel needs all ceil(V/8) CTAs resident at once; returns
 // EPHMC_ERR_UNSUPPORTED (nothing launched) when they are not, or V > 1024.
 int run_dataflow(double *M, LUWork &w, cudaStream_t st) {
     const int V = w.V;
     if (V > 1024 || w.sync == nullptr) return EPHMC_ERR_UNSUPPORTED;
     const int nblk = (V + kLuPanel - 1) / kLuPanel;
-    const int T = (V + 31) / 32 * 32;
-    int dev = 0, sms = 0, coop = 0, per_sm = 0;
+    int dev = 0, sms = 0, coop = 0;
     EPHMC_CUDA(cudaGetDevice(&dev));
     EPHMC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     EPHMC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-    EPHMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_dataflow<kLuPanel>, T, 0));
-    if (!coop || (long)per_sm * sms < nblk) return EPHMC_ERR_UNSUPPORTED;
-    double *panels = w.X;
-    void *args[] = {&M, (void *)&V, &panels, &w.ipiv, &w.diag, &w.info, &w.sync};
-    EPHMC_CUDA(cudaLaunchCooperativeKernel((const void *)k_gj_dataflow<kLuPanel>, dim3(nblk), dim3(T), args, 0, st));
-    ephmc::count_launch(1);
-    return EPHMC_OK;
+    if (!coop) return EPHMC_ERR_UNSUPPORTED;
+    // rows per thread: at most 256 threads (8 warps) per CTA
+    const int rpt = V <= 256 ? 1 : V <= 512 ? 2 : 4;
+    const int T = ((V + rpt - 1) / rpt + 31) / 32 * 32;
+    if (rpt == 1) return launch_dataflow<1>(M, w, nblk, T, sms, st);
+    if (rpt == 2) return launch_dataflow<2>(M, w, nblk, T, sms, st);
+    return launch_dataflow<4>(M, w, nblk, T, sms, st);
 }
 
 }  // namespace
