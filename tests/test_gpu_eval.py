@@ -192,3 +192,8 @@ def test_cfg1_fifty_configurations(gpu, restated):
         for mode in ("reference", "adjoint"):
             ld, pd = ctx.eval(x, mode=mode)
             assert rel(pd, g["force_seed1"]) <= tol, mode
+        ld, pd = ctx.eval(x, mode="mixed")
+        assert abs(ld - g["logdet"][0]) <= 1e-12 * abs(g["logdet"][0])
+        err = rel(pd, g["force_seed1"])
+        print(f"cfg1 seed 1: mixed force max-norm rel err {err:.2e}")
+        assert err <= 1e-2
