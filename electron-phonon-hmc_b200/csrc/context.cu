@@ -399,9 +399,6 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
             rc = launch_adjoint_sweep<double, double>(xd, c->c, c->lat, static_cast<const double *>(c->qstack), y0,
                                                       (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
                                                       c->stream);
-        else if (adjoint_rows_supported(c->lat))
-            rc = launch_adjoint_rows(xd, c->c, c->lat, static_cast<const float *>(c->qstack), y0, (int)c->nt,
-                                     c->flavors, f.single_particle, logdet, c->force, c->hop32, c->stream);
         else
             rc = launch_adjoint_sweep<float, float>(xd, c->c, c->lat, static_cast<const float *>(c->qstack), y0,
                                                     (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
@@ -472,8 +469,7 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     cudaSetDevice(c->device);
     void *bufs[] = {c->x,         c->force,        c->M,          c->G,        c->A,
                     c->B,         c->qstack,       c->jobs,       c->lat.ev_src, c->lat.ev_fac,
-                    c->lat.nbr,   c->lat.rev,      c->scratch,    c->work,     c->cc_part,
-                    c->hop32};
+                    c->lat.nbr,   c->lat.rev,      c->scratch,    c->work,     c->cc_part};
     for (void *b : bufs)
         if (b) cudaFree(b);
     lu_free(c->lu);
@@ -511,15 +507,6 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     c->nnt.resize(12 * (size_t)V);
     if (nnt_in) std::memcpy(c->nnt.data(), nnt_in, sizeof(unsigned) * 12 * V);
     else triangular_lattice(l1, l2, c->nnt.data());
-    if (nnt_in && l1 == 0 && V % 32 == 0) {
-        // a table that is construct_triangular(32, V/32) gets the lattice-structured kernels
-        std::vector<unsigned> canon(12 * (size_t)V);
-        triangular_lattice(32, V / 32, canon.data());
-        if (canon == c->nnt) {
-            c->l1 = l1 = 32;
-            c->l2 = l2 = V / 32;
-        }
-    }
     std::vector<int> es, ef, nb;
     int rc = build_event_tables(c->nnt.data(), (int)V, es, ef, nb);
     if (rc) {
@@ -560,7 +547,6 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     ALLOC(c->qstack, c->qstack_bytes);
     ALLOC(c->jobs, sizeof(SliceJob) * c->jobs_cap);
     ALLOC(c->scratch, sizeof(double) * c->scratch_n);
-    if (adjoint_rows_supported(c->lat)) ALLOC(c->hop32, sizeof(float) * adjoint_rows_scratch_floats((int)V, (int)nt));
 #undef ALLOC
     if (lu_alloc(c->lu, (int)V) != EPHMC_OK) {
         ephmc_ctx_destroy(c);

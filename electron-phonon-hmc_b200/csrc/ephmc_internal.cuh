@@ -99,14 +99,6 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
                          const QT *qstack, const double *Minv, int nt, unsigned flavors,
                          int single_particle, double logdet, double *force, cudaStream_t st);
 
-// FP32 adjoint sweep 2 for L1 = 32 lattices, one warp per vector (adjoint_rows.cu)
-// scratch: adjoint_rows_scratch_floats(V, nt) device floats (FP32 hopping tables)
-bool adjoint_rows_supported(const LatticeDev &lat);
-size_t adjoint_rows_scratch_floats(int V, int nt);
-int launch_adjoint_rows(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
-                        const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
-                        double *force, float *scratch, cudaStream_t st);
-
 // ---------------------------------------------------------------- drop-in helpers (helpers.cu)
 // out = (mu + K) in on nvec rows (or columns) of V x V matrices, reference order;
 // add_in: out = in + (mu + K) in (apply_K_plus_1_v)
@@ -212,6 +204,5 @@ struct ephmc_ctx {
     double *work = nullptr;     // 4 V*V doubles: full-matrix refinement and drop-in staging
     double *cc_part = nullptr;  // nt * V * 9 doubles: correlator partial sums
     double *scratch = nullptr;  // small device scratch (Fourier mode tables, reductions)
-    float *hop32 = nullptr;     // FP32 hopping tables of all slices (row-pipeline kernels)
     size_t scratch_n = 0;
 };
