@@ -160,6 +160,23 @@ def run_reference_arm(args):
     return 0
 
 
+def max_over_ranks(value, dist, device):
+    """The largest of `value` over all ranks (the slowest replica sets the
+    whole-job time); `value` itself when not distributed."""
+    if dist is None:
+        return float(value)
+    import torch
+    tt = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def whole_job_rate(n_ranks, steps, max_seconds):
+    """Evaluations per second of all replicas together: every rank runs
+    `steps` evaluations; the job takes as long as its slowest rank."""
+    return n_ranks * steps / max_seconds
+
+
 def load_ncu_summary():
     p = os.path.join(ROOT, "profiles", "ncu_summary.json")
     if os.path.exists(p):
@@ -238,12 +255,9 @@ def main():
             sampler.__exit__()
         launches = lib.ephmc_launch_count() - launches0
         ms = [a.elapsed_time(b) for a, b in ev]
-        total_ms = sum(ms)
-        if dist is not None:
-            tt = torch.tensor([total_ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            total_ms = float(tt.item())
-        results[path] = {"ms_per_step": total_ms / K, "value": ws * K / (total_ms / 1e3), "launches": launches,
+        total_ms = max_over_ranks(sum(ms), dist, dev)
+        results[path] = {"ms_per_step": total_ms / K, "value": whole_job_rate(ws, K, total_ms / 1e3),
+                         "launches": launches,
                          "clocks": sampler.summary() if sampler else None}
         phase[path] = {"mhat_ms": statistics.median(p[0] for p in ph), "lu_ms": statistics.median(p[1] for p in ph),
                        "force_ms": statistics.median(p[2] for p in ph)}
@@ -270,12 +284,9 @@ def main():
     t0 = time.perf_counter()
     for k in range(K):
         ctx.eval(xnp, pnp, mode=head)
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        tt = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e = {"value": ws * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * dim, "d2h_bytes_per_step": 8 * dim + 8}
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    e2e = {"value": whole_job_rate(ws, K, e2e_s), "unit": UNIT, "h2d_bytes_per_step": 8 * dim,
+           "d2h_bytes_per_step": 8 * dim + 8}
 
     line = None
     if rank == 0:
