@@ -117,6 +117,31 @@ def test_lu_against_numpy(gpu):
             assert np.array_equal(ipiv - 1, piv)
 
 
+@pytest.mark.parametrize("kind", ["permutation", "ones_plus_identity", "small_integers"])
+def test_lu_ties_follow_lapack(gpu, kind):
+    """Matrices with many equal magnitudes in a pivot column: the pivot rows
+    are dgetrf's (first logical row among equal magnitudes), so ipiv equals
+    scipy's LAPACK getrf and the inverse is exact to rounding."""
+    import ephmc
+    import scipy.linalg as sl
+    rng = np.random.default_rng(11)
+    V = 16
+    if kind == "permutation":
+        A = np.eye(V)[rng.permutation(V)]
+    elif kind == "ones_plus_identity":
+        A = np.ones((V, V)) + np.eye(V)
+    else:
+        A = rng.integers(-2, 3, size=(V, V)).astype(float) + 6 * np.eye(V)
+    with ephmc.Context(4, 4, 1, [0.1, 0.1, 0.1], [0, 0, 0], -1.0, 0.1) as ctx:
+        M = A.copy()
+        ld, sign, ipiv = ctx.logdet_inverse(M)
+    _, piv = sl.lu_factor(A.T)
+    assert np.array_equal(ipiv - 1, piv)
+    s_np, ld_np = np.linalg.slogdet(A.T)
+    assert sign == int(s_np) and abs(ld - ld_np) <= 1e-12 * max(1.0, abs(ld_np))
+    assert np.max(np.abs(M - np.linalg.inv(A))) <= 1e-12 * np.max(np.abs(np.linalg.inv(A)))
+
+
 def test_lu_singular_reports_status(gpu):
     import ephmc
     V = 16
