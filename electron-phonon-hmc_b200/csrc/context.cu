@@ -216,6 +216,11 @@ int build_M_hat(ephmc_ctx *c, const double *x, void *stack, bool stack_float, do
     std::vector<SliceJob> v{j};
     int rc = upload_jobs(c, v, c->jobs);
     if (rc) return rc;
+    // the adjoint paths (those with a stack) take the register-strip kernel where
+    // the lattice allows; the reference path keeps the reference's summation order
+    if (stack && slices_strip_supported(c->lat))
+        return stack_float ? launch_slices_strip<float>(x, c->c, c->lat, c->jobs, 1, c->stream)
+                           : launch_slices_strip<double>(x, c->c, c->lat, c->jobs, 1, c->stream);
     if (stack && stack_float)
         return launch_slices<double, double, float>(Axis::Rows, x, c->c, c->lat, c->jobs, 1, c->stream);
     return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs, 1, c->stream);

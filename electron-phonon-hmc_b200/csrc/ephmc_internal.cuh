@@ -83,6 +83,14 @@ template <typename Real, typename Store, typename StackT>
 int launch_slices(Axis axis, const double *x, const Couplings &c, const LatticeDev &lat,
                   const SliceJob *jobs_dev, int njobs, cudaStream_t st);
 
+// Same jobs on rows (identity or src start, Rows axis only) for L1 = 32
+// lattices with the lattice in registers (slices_strip.cu); sums in a
+// different order from launch_slices, so results agree to rounding.
+bool slices_strip_supported(const LatticeDev &lat);
+template <typename StackT>
+int launch_slices_strip(const double *x, const Couplings &c, const LatticeDev &lat, const SliceJob *jobs_dev,
+                        int njobs, cudaStream_t st);
+
 // Reference-algorithm refinement + link contraction for slices t0..t0+nb-1:
 //   A_t = pair 1 on columns of G_t, B_t = pair 0 on rows of G_t (already formed),
 //   force[t][i][k] from the link entries of
