@@ -404,6 +404,9 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
             rc = launch_adjoint_sweep<double, double>(xd, c->c, c->lat, static_cast<const double *>(c->qstack), y0,
                                                       (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
                                                       c->stream);
+        else if (adjoint_strip_supported(c->lat))
+            rc = launch_adjoint_strip(xd, c->c, c->lat, static_cast<const float *>(c->qstack), y0, (int)c->nt,
+                                      c->flavors, f.single_particle, logdet, c->force, c->stream);
         else
             rc = launch_adjoint_sweep<float, float>(xd, c->c, c->lat, static_cast<const float *>(c->qstack), y0,
                                                     (int)c->nt, c->flavors, f.single_particle, logdet, c->force,

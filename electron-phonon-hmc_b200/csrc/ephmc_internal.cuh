@@ -107,6 +107,13 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
                          const QT *qstack, const double *Minv, int nt, unsigned flavors,
                          int single_particle, double logdet, double *force, cudaStream_t st);
 
+// FP32 adjoint sweep 2 for L1 = 32 lattices with the lattice in registers
+// (adjoint_strip.cu)
+bool adjoint_strip_supported(const LatticeDev &lat);
+int launch_adjoint_strip(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
+                         const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
+                         double *force, cudaStream_t st);
+
 // ---------------------------------------------------------------- drop-in helpers (helpers.cu)
 // out = (mu + K) in on nvec rows (or columns) of V x V matrices, reference order;
 // add_in: out = in + (mu + K) in (apply_K_plus_1_v)
