@@ -43,6 +43,10 @@ FLOP_PER_EVAL = V * V * NT * (84 * (1 + 6) + 170) + 2 * V ** 3
 # adjoint force sweep (one launch): per vector, site and slice 7 stencils (7 FMA each),
 # 3 pair combinations, link contraction (3 links x 8 products) ~ 173 flop
 ADJ_SWEEP_FLOP = 173 * V * V * NT
+# sweep 1 (M_hat and the q stack): Nt slice applications of 84 flop per site and vector
+SWEEP1_FLOP = 84 * V * V * NT
+# LU + inverse (getrf + getri): 2 V^3
+LU_FLOP = 2 * V ** 3
 
 
 def dist_env():
@@ -293,16 +297,32 @@ def main():
         fp32 = C_float_peak(lib, False)
         fp64 = C_float_peak(lib, True)
         ncu = load_ncu_summary()
-        # dominant kernel of the headline path: the adjoint force sweep (one launch per eval)
-        fms = phase[head]["force_ms"]
-        ach = ADJ_SWEEP_FLOP / (fms * 1e-3) / 1e12 if fms > 0 else None
-        peak = fp32 if head == "mixed" else fp64
-        roofline = {"bound": "fp32" if head == "mixed" else "fp64", "kernel": "k_adjoint (force sweep)",
-                    "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                    "frac": (ach / peak) if (ach and peak) else None,
-                    "peak_source": "measured in this run (CUDA-core FMA probe, ephmc_measure_fma_peak)",
-                    "traffic": ncu.get("k_adjoint_dram_bytes_per_launch"),
-                    "algorithmic_flop_per_launch": ADJ_SWEEP_FLOP}
+        # per kernel of the headline path: algorithmic flop per launch / in-run duration
+        ph = phase[head]
+        sweep_peak = fp32 if head == "mixed" else fp64
+
+        def frac(flop, ms, peak):
+            ach = flop / (ms * 1e-3) / 1e12 if ms > 0 else None
+            return ach, (ach / peak if (ach and peak) else None)
+
+        kernels = {}
+        for name, flop, ms, pk, bound in (
+                ("k_gj_dataflow (LU, inverse, log det)", LU_FLOP, ph["lu_ms"], fp64, "fp64"),
+                ("k_adjoint_strip (force sweep)" if head == "mixed" else "k_adjoint (force sweep)",
+                 ADJ_SWEEP_FLOP, ph["force_ms"], sweep_peak, "fp32" if head == "mixed" else "fp64"),
+                ("k_slices_strip (M_hat + q stack)", SWEEP1_FLOP, ph["mhat_ms"], fp64, "fp64")):
+            ach, fr = frac(flop, ms, pk)
+            kernels[name] = {"ms": ms, "achieved_tflops": ach, "peak_tflops": pk, "frac": fr, "bound": bound,
+                             "algorithmic_flop_per_launch": flop}
+        # the dominant kernel (largest share of the step) is the LU
+        ach, fr = frac(LU_FLOP, ph["lu_ms"], fp64)
+        roofline = {"bound": "fp64", "kernel": "k_gj_dataflow (LU + inverse + log det, one cooperative launch)",
+                    "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": fr,
+                    "peak_source": "measured in this run (CUDA-core FP64 FMA probe, ephmc_measure_fma_peak)",
+                    "traffic": ncu.get("k_gj_dataflow_dram_bytes_per_launch"),
+                    "algorithmic_flop_per_launch": LU_FLOP,
+                    "note": "latency-bound: 1024 sequential pivot steps and 127 panel hand-offs",
+                    "kernels": kernels}
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
             try:

@@ -195,7 +195,13 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     const size_t fac_b = 3 * (size_t)V * sizeof(Real);
     const size_t budget = 200 * 1024;
     int R = (int)((budget - fac_b) / per_vec);
-    if (R < 1) return EPHMC_ERR_UNSUPPORTED;
+    if (R < 1 || fac_b + per_vec > budget) {
+        set_status(EPHMC_ERR_UNSUPPORTED, sizeof(Real) == 8
+                                              ? "adjoint sweep: nine FP64 vectors of V sites exceed shared memory "
+                                                "(V > 2048); use the mixed or the reference force"
+                                              : "adjoint sweep: nine FP32 vectors of V sites exceed shared memory");
+        return EPHMC_ERR_UNSUPPORTED;
+    }
     if (R > 4) R = 4;
     const size_t smem = per_vec * R + fac_b;
     double pref = (double)flavors;

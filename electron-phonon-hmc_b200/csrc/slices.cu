@@ -188,7 +188,10 @@ int launch_axis(const double *x, const Couplings &c, const LatticeDev &lat, cons
                 int njobs, cudaStream_t st) {
     const int V = lat.V;
     Shape sh = pick_shape(V);
-    if (sh.smem > 227 * 1024) return EPHMC_ERR_UNSUPPORTED;
+    if (sh.smem > 227 * 1024) {
+        set_status(EPHMC_ERR_UNSUPPORTED, "slice propagation: a vector and its stencil image exceed shared memory");
+        return EPHMC_ERR_UNSUPPORTED;
+    }
     dim3 grid((V + sh.R - 1) / sh.R, njobs);
     void (*kern)(const double *, Couplings, const int *, const int *, const SliceJob *, int, int) = nullptr;
     switch (sh.S) {
