@@ -6,6 +6,8 @@
 //   evolve_bosons          (simulation/organic_bosons.c:126-150)
 //   sample_fourier_momenta (:76-100), sample_free_bosons (:55-74)
 //   energy_fourier_momenta (:102-124)
+//   evolve_bosons_approx_step (:152-177), the kinetic step of classical
+//   Fourier acceleration
 // Here one kernel does transform -> per-mode update -> inverse transform for a
 // tile of 32 series held in shared memory, so x and p are read and written
 // once (HBM-bound: 2 x 8 x 3V x Nt bytes in, the same out).  The transform is
@@ -67,7 +69,8 @@ __device__ void load_twiddles(double *cs, double *sn, int n) {
     }
 }
 
-// mode: 0 evolve (x,p), 1 scale p by modes[k] (momentum refresh), 2 scale x by modes[k] (free bosons)
+// mode: 0 evolve (x,p), 1 scale p by modes[k] (momentum refresh), 2 scale x by modes[k] (free bosons),
+// 3 x <- (x + modes[k] p) c mode by mode, p read only (classical acceleration's kinetic step)
 __global__ void k_fa(double *__restrict__ x, double *__restrict__ p, int ld, int n, const double *__restrict__ mc,
                      const double *__restrict__ ms, double c, int mode) {
     extern __shared__ double sm[];
@@ -101,6 +104,10 @@ __global__ void k_fa(double *__restrict__ x, double *__restrict__ p, int ld, int
         } else if (mode == 1) {
             pr[o] *= mc[k];
             pi[o] *= mc[k];
+        } else if (mode == 3) {
+            // xc += (h / freq2) pc ; xc *= 1/n   (:170-173)
+            xr[o] = fma(mc[k], pr[o], xr[o]) * c;
+            xi[o] = fma(mc[k], pi[o], xi[o]) * c;
         } else {
             xr[o] *= mc[k];
             xi[o] *= mc[k];
@@ -108,12 +115,12 @@ __global__ void k_fa(double *__restrict__ x, double *__restrict__ p, int ld, int
     }
     __syncthreads();
     if (mode != 1) dft_inv(xr, xi, ax, n, cs, sn, e);
-    if (mode != 2) dft_inv(pr, pi, ap, n, cs, sn, e);
+    if (mode != 2 && mode != 3) dft_inv(pr, pi, ap, n, cs, sn, e);
     __syncthreads();
     if (valid) {
         for (int t = threadIdx.y; t < n; t += kRowsY) {
             if (mode != 1) x[(size_t)t * ld + e0 + e] = ax[t * kTile + e];
-            if (mode != 2) p[(size_t)t * ld + e0 + e] = ap[t * kTile + e];
+            if (mode != 2 && mode != 3) p[(size_t)t * ld + e0 + e] = ap[t * kTile + e];
         }
     }
 }
@@ -196,6 +203,27 @@ int fa_evolve(double *x, double *p, int ld, int n, double omega, double h, doubl
     const size_t smem = fa_smem(n, true);
     EPHMC_CUDA(cudaFuncSetAttribute(k_fa, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_fa<<<(ld + kTile - 1) / kTile, dim3(kTile, kRowsY), smem, st>>>(x, p, ld, n, d, d + nc, c, 0); ephmc::count_launch(1);
+    EPHMC_CUDA(cudaGetLastError());
+    return EPHMC_OK;
+}
+
+// x <- x + inverse transform of (h / freq2_k) P_k, normalised by 1/n
+// (evolve_bosons_approx_step, simulation/organic_bosons.c:152-177); omega is
+// the accelerated frequency sqrt(cfa_mass^2 + omega^2) the caller passes
+int fa_approx_step(double *x, const double *p, int ld, int n, double omega, double h, double *scratch,
+                   cudaStream_t st) {
+    if (n < 1 || n > 512) return EPHMC_ERR_UNSUPPORTED;
+    const int nc = n / 2 + 1;
+    std::vector<double> tab(nc);
+    for (int k = 0; k < nc; ++k) tab[k] = h / freq2(omega, k, n);  // inv_mass (:167)
+    double *d = nullptr;
+    int rc = upload_modes(tab, scratch, st, &d);
+    if (rc) return rc;
+    const size_t smem = fa_smem(n, true);
+    EPHMC_CUDA(cudaFuncSetAttribute(k_fa, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_fa<<<(ld + kTile - 1) / kTile, dim3(kTile, kRowsY), smem, st>>>(x, const_cast<double *>(p), ld, n, d, d,
+                                                                      1.0 / n, 3);
+    ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
     return EPHMC_OK;
 }

@@ -183,6 +183,11 @@ size_t fa_scratch_doubles(int ld, int nt);
 int fa_evolve(double *x, double *p, int ld, int nt, double omega, double h, double *scratch, cudaStream_t st);
 int fa_scale_modes(double *v, int ld, int nt, double omega, int mode, double *scratch, cudaStream_t st);
 int fa_energy(const double *p, int ld, int nt, double omega, double *out_dev, double *scratch, cudaStream_t st);
+int fa_approx_step(double *x, const double *p, int ld, int nt, double omega, double h, double *scratch,
+                   cudaStream_t st);
+// update_x of classical Fourier acceleration (simulation/organic_hmc.c:142-163)
+// on device buffers of the context's shape; p_dot is scratch for the boson force
+int classical_update_x(ephmc_ctx *c, double *x, double *p, double *p_dot, double h, double half);
 
 }  // namespace ephmc
 

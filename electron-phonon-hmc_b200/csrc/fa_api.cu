@@ -153,6 +153,24 @@ int ephmc_fa_energy(ephmc_ctx *c, const double *p, double *energy) {
     return EPHMC_OK;
 }
 
+// evolve_bosons_approx_step (simulation/organic_bosons.c:152-177): x moves by
+// h times the accelerated velocity, mode by mode, at frequency
+// sqrt(cfa_mass^2 + omega^2) when CLASSICAL_FOURIER_ACC is set
+int ephmc_fa_approx_step(ephmc_ctx *c, double *x, const double *p, double h) {
+    if (!c || !x || !p) return fail(EPHMC_ERR_ARG, "ephmc_fa_approx_step");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t dim = (size_t)c->nt * c->V * 3;
+    Staged sx{}, sp{};
+    int rc;
+    if ((rc = stage(c, x, c->x, dim, sx))) return rc;
+    if ((rc = stage(c, const_cast<double *>(p), c->force, dim, sp))) return rc;
+    double om = c->omega;
+    if (c->flags.classical_fourier_acc) om = std::sqrt(c->flags.cfa_mass * c->flags.cfa_mass + om * om);
+    if ((rc = fa_approx_step(sx.d, sp.d, 3 * (int)c->V, (int)c->nt, om, h, c->scratch, c->stream)))
+        return fail(rc, "fa_approx_step");
+    return unstage(c, sx, dim);
+}
+
 // hamilton (simulation/organic_hmc.c:67-84)
 int ephmc_hamilton(ephmc_ctx *c, const double *x, double logdet, double energyP, double *H) {
     if (!c || !x || !H) return fail(EPHMC_ERR_ARG, "ephmc_hamilton");
@@ -176,3 +194,44 @@ int ephmc_hamilton(ephmc_ctx *c, const double *x, double logdet, double energyP,
 }
 
 }  // extern "C"
+
+namespace ephmc {
+
+// update_x with CLASSICAL_FOURIER_ACC (simulation/organic_hmc.c:142-163): the
+// leapfrog step h is split into cfa_steps sub-steps of the harmonic boson
+// force (plain omega) and the accelerated kinetic step (accelerated omega);
+// half = 0.5 is the first half step, -0.5 the last, 1 a full step.  x, p,
+// p_dot: device buffers of the context's shape, on the context's stream.
+int classical_update_x(ephmc_ctx *c, double *x, double *p, double *p_dot, double h, double half) {
+    const int ld = 3 * (int)c->V, nt = (int)c->nt;
+    const size_t dim = (size_t)nt * ld;
+    const unsigned steps = c->flags.cfa_steps ? c->flags.cfa_steps : 1;
+    double om = c->omega;
+    const double om_acc = std::sqrt(c->flags.cfa_mass * c->flags.cfa_mass + om * om);
+    h /= steps;
+    int rc;
+    auto kick = [&](double w) -> int {  // p += w * (boson force at x)
+        int r = launch_boson_force(x, p_dot, om, ld, nt, true, c->stream);
+        return r ? r : launch_axpy(p, p_dot, w, dim, c->stream);
+    };
+    auto drift = [&](double w) { return fa_approx_step(x, p, ld, nt, om_acc, w, c->scratch, c->stream); };
+    if (half != .5) {
+        if ((rc = kick(.5 * h))) return rc;
+        for (unsigned k = 0; k < steps / 2; ++k) {
+            if ((rc = drift(h))) return rc;
+            if ((rc = kick(h))) return rc;
+        }
+        if ((rc = drift(.5 * h))) return rc;
+    }
+    if (half != -.5) {
+        if ((rc = drift(.5 * h))) return rc;
+        for (unsigned k = 0; k < steps / 2; ++k) {
+            if ((rc = kick(h))) return rc;
+            if ((rc = drift(h))) return rc;
+        }
+        if ((rc = kick(.5 * h))) return rc;
+    }
+    return EPHMC_OK;
+}
+
+}  // namespace ephmc

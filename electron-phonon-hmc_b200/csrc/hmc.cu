@@ -114,7 +114,13 @@ double kinetic(ephmc_ctx *c, double *p_dev, size_t dim) {
     return e;
 }
 
-void update_x_dev(ephmc_ctx *c, double *x, double *p, size_t dim, double h, double half) {
+void update_x_dev(ephmc_ctx *c, double *x, double *p, double *p_dot, size_t dim, double h, double half) {
+    if (c->flags.classical_fourier_acc && !c->flags.no_fourier_acc) {
+        if (classical_update_x(c, x, p, p_dot, h, half) != EPHMC_OK)
+            std::fprintf(stderr, "ephmc update_x: %s\n", ephmc_last_error_message());
+        cudaStreamSynchronize(c->stream);
+        return;
+    }
     if (c->flags.no_fourier_acc) {
         launch_axpy(x, p, h * std::fabs(half), dim, c->stream);
         cudaStreamSynchronize(c->stream);
@@ -130,7 +136,7 @@ void leap_frog_dev(ephmc_ctx *c, double *x, double *p, double *p_dot, double *M_
     const size_t dim = (size_t)c->nt * c->V * 3, VV = (size_t)c->V * c->V;
     const double h = steps ? traj_length / steps : 2 * traj_length;
     double half = .5;
-    update_x_dev(c, x, p, dim, h, half);
+    update_x_dev(c, x, p, p_dot, dim, h, half);
     half = 1;
     for (unsigned s = 1; s <= steps; ++s) {
         double ld = 0;
@@ -140,7 +146,7 @@ void leap_frog_dev(ephmc_ctx *c, double *x, double *p, double *p_dot, double *M_
         cudaMemcpyAsync(M_hat, c->M, sizeof(double) * VV, cudaMemcpyDeviceToDevice, c->stream);
         launch_axpy(p, p_dot, h, dim, c->stream);
         if (s == steps) half = -.5;
-        update_x_dev(c, x, p, dim, h, half);
+        update_x_dev(c, x, p, p_dot, dim, h, half);
     }
     cudaStreamSynchronize(c->stream);
 }

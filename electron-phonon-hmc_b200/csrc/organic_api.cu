@@ -587,7 +587,15 @@ double energy_fourier_momenta(ephmc_dcomplex *, double omega, unsigned ns, unsig
     if (!fft || !fft[1]) return NAN;
     ephmc_ctx *c = fa_ctx(ns, nt, omega);
     double e = NAN;
-    if (!c || ephmc_fa_energy(c, static_cast<double *>(fft[1]->in), &e) != EPHMC_OK) report("energy_fourier_momenta");
+    if (!c) {
+        report("energy_fourier_momenta");
+        return e;
+    }
+    // omega is used as given (energy_momenta passes the accelerated one)
+    ephmc_flags f = c->flags;
+    f.classical_fourier_acc = 0;
+    ephmc_ctx_set_flags(c, &f);
+    if (ephmc_fa_energy(c, static_cast<double *>(fft[1]->in), &e) != EPHMC_OK) report("energy_fourier_momenta");
     return e;
 }
 // evolve_bosons (:126-150): x and p are the buffers of plans 0 and 1
@@ -597,11 +605,15 @@ void evolve_bosons(ephmc_dcomplex *, double omega, unsigned ns, unsigned, unsign
     if (!c || ephmc_fa_evolve(c, static_cast<double *>(fft[0]->in), static_cast<double *>(fft[1]->in), h) != EPHMC_OK)
         report("evolve_bosons");
 }
-// evolve_bosons_approx_step (:152-177): classical Fourier acceleration is not on the GPU path
-void evolve_bosons_approx_step(ephmc_dcomplex *, double, unsigned, unsigned, unsigned, const fftw_plan *, double,
-                               organic_flags *) {
-    set_status(EPHMC_ERR_UNSUPPORTED, "CLASSICAL_FOURIER_ACC is not implemented on the GPU path");
-    report("evolve_bosons_approx_step");
+// evolve_bosons_approx_step (:152-177): x and p are the buffers of plans 0 and 1
+void evolve_bosons_approx_step(ephmc_dcomplex *, double omega, unsigned ns, unsigned, unsigned nt,
+                               const fftw_plan *fft, double h, organic_flags *mode) {
+    if (!fft || !fft[0] || !fft[1]) return;
+    ephmc_ctx *c = fa_ctx(ns, nt, omega);
+    if (!c) return report("evolve_bosons_approx_step");
+    ephmc_ctx_set_flags(c, mode);
+    if (ephmc_fa_approx_step(c, static_cast<double *>(fft[0]->in), static_cast<double *>(fft[1]->in), h) != EPHMC_OK)
+        report("evolve_bosons_approx_step");
 }
 // boson_force (:179-194)
 void boson_force(double *x, double *p_dot, double omega, unsigned ns, unsigned nn, unsigned nt, int overwrite) {
@@ -703,7 +715,6 @@ double check_force(double *x, double *p, double *p_dot, double *M_hat, double *w
 // update_x (:136-165)
 void update_x(double *x, double *p, double *p_dot, ephmc_dcomplex *xc, double omega, unsigned ns, unsigned nn,
               unsigned nt, const fftw_plan *fft, double h, double half, organic_flags *mode) {
-    (void)p_dot;
     (void)xc;
     (void)fft;
     const size_t dim = (size_t)nt * ns * nn / 2;
@@ -715,8 +726,16 @@ void update_x(double *x, double *p, double *p_dot, ephmc_dcomplex *xc, double om
         return;
     }
     if (mode && mode->classical_fourier_acc) {
-        set_status(EPHMC_ERR_UNSUPPORTED, "CLASSICAL_FOURIER_ACC is not implemented on the GPU path");
-        return report("update_x");
+        ephmc_ctx *c = fa_ctx(ns, nt, omega);
+        if (!c) return report("update_x");
+        ephmc_ctx_set_flags(c, mode);
+        DView X(x, dim), P(p, dim), PD(p_dot, dim);
+        if (classical_update_x(c, X.d, P.d, PD.d, h, half) != EPHMC_OK) return report("update_x");
+        cudaStreamSynchronize(c->stream);
+        X.back();
+        P.back();
+        PD.back();
+        return;
     }
     ephmc_ctx *c = fa_ctx(ns, nt, omega);
     if (!c || ephmc_fa_evolve(c, x, p, std::fabs(half) * h) != EPHMC_OK) report("update_x");

@@ -81,6 +81,7 @@ def load_library(path: str | None = None, build_if_missing: bool = True):
     sig("ephmc_ctx_get_inverse", _I, [_P, _P])
     sig("ephmc_ctx_last_timings", _I, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)])
     sig("ephmc_fa_evolve", _I, [_P, _P, _P, _D])
+    sig("ephmc_fa_approx_step", _I, [_P, _P, _P, _D])
     sig("ephmc_fa_scale_momenta", _I, [_P, _P])
     sig("ephmc_fa_scale_free_bosons", _I, [_P, _P])
     sig("ephmc_fa_energy", _I, [_P, _P, C.POINTER(_D)])

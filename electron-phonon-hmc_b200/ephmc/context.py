@@ -143,6 +143,10 @@ class Context:
     def fa_evolve(self, x, p, h):
         check(self.lib.ephmc_fa_evolve(self.h, ptr(x), ptr(p), float(h)), "ephmc_fa_evolve")
 
+    def fa_approx_step(self, x, p, h):
+        """Kinetic step of classical Fourier acceleration (x in place)."""
+        check(self.lib.ephmc_fa_approx_step(self.h, ptr(x), ptr(p), float(h)), "ephmc_fa_approx_step")
+
     def fa_scale_momenta(self, p):
         check(self.lib.ephmc_fa_scale_momenta(self.h, ptr(p)), "ephmc_fa_scale_momenta")
 

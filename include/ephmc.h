@@ -195,6 +195,12 @@ EPHMC_API int ephmc_fa_scale_momenta(ephmc_ctx *ctx, double *p);
 EPHMC_API int ephmc_fa_scale_free_bosons(ephmc_ctx *ctx, double *x);
 /* Kinetic energy of p in Fourier space (energy_fourier_momenta, :102-124). */
 EPHMC_API int ephmc_fa_energy(ephmc_ctx *ctx, const double *p, double *energy);
+/* Kinetic step of classical Fourier acceleration: x += h * (p divided per
+ * Matsubara mode by omega + (2 sin(pi k/Nt))^2/omega, at the accelerated
+ * omega sqrt(cfa_mass^2 + omega^2) when the context's flags set
+ * CLASSICAL_FOURIER_ACC); p is not changed (evolve_bosons_approx_step,
+ * simulation/organic_bosons.c:152-177). */
+EPHMC_API int ephmc_fa_approx_step(ephmc_ctx *ctx, double *x, const double *p, double h);
 /* Action -flavors*logdet + energyP + (sum (dx_t)^2/omega + omega sum x^2)/2
  * (hamilton, simulation/organic_hmc.c:67-84). */
 EPHMC_API int ephmc_hamilton(ephmc_ctx *ctx, const double *x, double logdet, double energyP, double *H);

@@ -267,6 +267,8 @@ class Reference(_Lib):
         s("ref_fa_sample_momenta", None, [_P, _D, _P])
         s("ref_fa_energy", _D, [_P, _D])
         s("ref_fa_sample_free", None, [_P, _D])
+        s("ref_fa_approx_step", None, [_P, _D, _D, _D])
+        s("ref_fa_update_x", None, [_P, _P, _D, _D, _D, _P, _U, _D])
         s("ref_higher_matsubaras_norm", _D, [_P, _U, _U])
         s("ref_boson_force", None, [_P, _P, _D, _U, _U, _I])
         s("ref_run_main", _I, [C.c_ulong, C.c_char_p, C.c_char_p, C.c_char_p])
@@ -417,6 +419,14 @@ class RefFA:
 
     def energy(self, omega):
         return self.ref.lib.ref_fa_energy(self.h, omega)
+
+    def approx_step(self, omega, h, cfa_mass):
+        self.ref.lib.ref_fa_approx_step(self.h, omega, h, cfa_mass)
+
+    def update_x(self, omega, h, half, flags=(0,) * 7, cfa_steps=1, cfa_mass=0.0):
+        p_dot = np.zeros(3 * self.ns * self.nt)
+        f = np.ascontiguousarray(flags, dtype=np.int32)
+        self.ref.lib.ref_fa_update_x(self.h, _ptr(p_dot), omega, h, half, _ptr(f), cfa_steps, cfa_mass)
 
     def sample_free(self, seed, omega):
         self.ref.lib.ref_init_genrand64(seed)

@@ -301,6 +301,29 @@ double ref_fa_energy(ref_fa *f, double omega) {
     return energy_fourier_momenta(f->xc + f->compl_dim, omega, f->ns, 6, f->nt, f->fft);
 }
 
+/* evolve_bosons_approx_step (simulation/organic_bosons.c:152-177) with
+ * CLASSICAL_FOURIER_ACC set and the given mass */
+void ref_fa_approx_step(ref_fa *f, double omega, double h, double cfa_mass) {
+    organic_flags m;
+    memset(&m, 0, sizeof(m));
+    m.classical_fourier_acc = 1;
+    m.cfa_steps = 1;
+    m.cfa_mass = cfa_mass;
+    evolve_bosons_approx_step(f->xc, omega, f->ns, 6, f->nt, f->fft, h, &m);
+}
+
+/* update_x (simulation/organic_hmc.c:136-165) on [x|p] with the given flags
+ * (as fill_flags reads them) and classical acceleration parameters; p_dot is
+ * caller scratch of dim doubles */
+void ref_fa_update_x(ref_fa *f, double *p_dot, double omega, double h, double half, const int *flags,
+                     unsigned cfa_steps, double cfa_mass) {
+    organic_flags m;
+    fill_flags(&m, flags);
+    m.cfa_steps = cfa_steps;
+    m.cfa_mass = cfa_mass;
+    update_x(f->xp, f->xp + f->dim, p_dot, f->xc, omega, f->ns, 6, f->nt, f->fft, h, half, &m);
+}
+
 /* sample_free_bosons (simulation/organic_bosons.c:55-74) */
 void ref_fa_sample_free(ref_fa *f, double omega) {
     sample_free_bosons(f->xp, f->xc, omega, f->ns, 6, f->nt, f->fft);

@@ -222,3 +222,42 @@ def test_cfg1_fifty_configurations(gpu, restated):
         err = rel(pd, g["force_seed1"])
         print(f"cfg1 seed 1: mixed force max-norm rel err {err:.2e}")
         assert err <= 1e-2
+
+
+@pytest.mark.parametrize("half", [0.5, 1.0, -0.5])
+def test_classical_fourier_acceleration_matches_reference(gpu, reference, half):
+    """CLASSICAL_FOURIER_ACC: the kinetic step (ephmc_fa_approx_step) and the
+    whole update_x of the drop-in surface (4 sub-steps of boson force and
+    kinetic step, simulation/organic_hmc.c:142-163) against the reference's,
+    for the first half step, a full step and the last half step."""
+    import ctypes as C
+
+    import ephmc
+    from oracle import RefFA
+    ns, nt, L = 16, 16, 4
+    omega, mass, steps, h = 0.37, 0.5, 4, 0.3
+    rng = np.random.default_rng(5)
+    x, p = rng.standard_normal(3 * ns * nt), rng.standard_normal(3 * ns * nt)
+    flags = {"classical_fourier_acc": 1, "cfa_steps": steps, "cfa_mass": mass}
+    # kinetic step alone
+    fa = RefFA(reference, ns, nt)
+    fa.set(x, p)
+    fa.approx_step(omega, h, mass)
+    xr, _ = fa.get()
+    with ephmc.Context(L, L, nt, [0.1, 0.1, 0.1], [0.01, 0.01, 0.01], -1.0, omega, flags=flags) as ctx:
+        xg = x.copy()
+        ctx.fa_approx_step(xg, p, h)
+    assert np.max(np.abs(xg - xr)) <= 1e-12 * np.max(np.abs(xr))
+    # update_x of the drop-in surface
+    fa.set(x, p)
+    fa.update_x(omega, h, half, flags=(0, 0, 0, 0, 0, 0, 1), cfa_steps=steps, cfa_mass=mass)
+    xr, pr = fa.get()
+    lib = ephmc.load_library()
+    f = ephmc._lib.Flags(classical_fourier_acc=1, cfa_steps=steps, cfa_mass=mass)
+    lib.update_x.restype = None
+    lib.update_x.argtypes = [C.c_void_p] * 4 + [C.c_double, C.c_uint, C.c_uint, C.c_uint, C.c_void_p, C.c_double,
+                                                 C.c_double, C.c_void_p]
+    xg, pg, pdot = x.copy(), p.copy(), np.zeros_like(x)
+    lib.update_x(xg.ctypes.data, pg.ctypes.data, pdot.ctypes.data, None, omega, ns, 6, nt, None, h, half, C.byref(f))
+    assert np.max(np.abs(xg - xr)) <= 1e-12 * np.max(np.abs(xr))
+    assert np.max(np.abs(pg - pr)) <= 1e-12 * np.max(np.abs(pr))

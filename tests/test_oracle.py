@@ -151,3 +151,26 @@ def test_restated_live_against_reference(restated, reference):
     assert np.array_equal(G, G_r), "log-depth sharing must be bit-identical given the same inverse"
     for t in (0, 3, 7):
         assert np.array_equal(restated.refine(m, x, G[t], t), ctx.refine(x, G_r[t], t))
+
+
+def test_reference_classical_acceleration_step_matches_its_formula(reference):
+    """The reference's evolve_bosons_approx_step (through oracle/ref_driver.c)
+    equals x + irfft((h / freq2_k) rfft(p)) per series, with
+    freq2_k = w + (2 sin(pi k / Nt))^2 / w and w = sqrt(cfa_mass^2 + omega^2)
+    (simulation/organic_bosons.c:152-177)."""
+    from oracle import RefFA
+    ns, nt = 4, 16
+    fa = RefFA(reference, ns, nt)
+    rng = np.random.default_rng(1)
+    ld = 3 * ns
+    x, p = rng.standard_normal(ld * nt), rng.standard_normal(ld * nt)
+    fa.set(x, p)
+    omega, h, mass = 0.3, 0.2, 0.5
+    fa.approx_step(omega, h, mass)
+    xr, pr = fa.get()
+    w = np.sqrt(mass ** 2 + omega ** 2)
+    k = np.arange(nt // 2 + 1)
+    f2 = w + (2 * np.sin(np.pi * k / nt)) ** 2 / w
+    xn = x.reshape(nt, ld) + np.fft.irfft((h / f2)[:, None] * np.fft.rfft(p.reshape(nt, ld), axis=0), n=nt, axis=0)
+    assert np.max(np.abs(xr - xn.ravel())) <= 1e-13
+    assert np.array_equal(pr, p)
