@@ -75,7 +75,7 @@ def build(force=False, verbose=False):
         msg = "\n".join(f"--- {s}\n{o}" for s, o in failed)
         raise RuntimeError(f"nvcc failed:\n{msg}")
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lcusolver", "-lcublas"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB

@@ -62,6 +62,11 @@ int build_event_tables(const unsigned *nnt, int V, std::vector<int> &ev_src,
                        std::vector<int> &ev_fac, std::vector<int> &nbr);
 void triangular_lattice(unsigned l1, unsigned l2, unsigned *nnt);
 
+// ---------------------------------------------------------------- static disorder (trans_loc.cu)
+int tl_create_nnt(ephmc_tl **out, const unsigned *nnt, unsigned V, unsigned nbins, const double t[3],
+                  const double kappa[3], double mu, const double contr_mat[6], unsigned lanes, int device);
+int tl_set_params(ephmc_tl *tl, const double t[3], const double kappa[3], double mu, const double contr_mat[6]);
+
 // ---------------------------------------------------------------- slice propagation
 // One job = one V x V matrix whose vectors (rows, or columns) get a sequence
 // of slice propagators, optionally spilling the state after each slice.

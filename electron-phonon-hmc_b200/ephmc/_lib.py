@@ -86,6 +86,12 @@ def load_library(path: str | None = None, build_if_missing: bool = True):
     sig("ephmc_fa_scale_free_bosons", _I, [_P, _P])
     sig("ephmc_fa_energy", _I, [_P, _P, C.POINTER(_D)])
     sig("ephmc_hamilton", _I, [_P, _P, _D, _D, C.POINTER(_D)])
+    sig("ephmc_tl_create", _I, [C.POINTER(_P), _U, _U, _U, _P, _P, _D, _P, _U, _I])
+    sig("ephmc_tl_destroy", _I, [_P])
+    sig("ephmc_tl_set_stream", _I, [_P, _P])
+    sig("ephmc_tl_default_width", _I, [_P, C.POINTER(_D)])
+    sig("ephmc_tl_run", _I, [_P, _P, _U, _D, _P, _P])
+    sig("ephmc_tl_last_timings", _I, [_P, C.POINTER(C.c_float)])
     sig("ephmc_alloc", _P, [C.c_size_t])
     sig("ephmc_free", None, [_P])
     sig("ephmc_device_synchronize", _I, [])

@@ -7,12 +7,13 @@
  *  1. The drop-in surface: the reference's own functions with identical names
  *     and prototypes (declared in ephmc_organic.h), so the reference's C host
  *     code links against this library in place of organic_dense_matrix.o,
- *     organic_hmc.o and organic_bosons.o.
+ *     organic_hmc.o, organic_bosons.o and organic_trans_loc.o.
  *
  *  2. The native surface below (prefix ephmc_): a device context that keeps
  *     the lattice, parameters and every work buffer resident on one GPU and
  *     evaluates log det M and the fermion force in one call, in one of three
- *     algorithms.
+ *     algorithms; and a static-disorder handle (ephmc_tl_) that bins the
+ *     current matrix elements of batches of disorder samples.
  *
  * Pointers: every double* argument of the native surface may be a device
  * pointer (used in place) or a host pointer (staged through the context's
@@ -204,6 +205,39 @@ EPHMC_API int ephmc_fa_approx_step(ephmc_ctx *ctx, double *x, const double *p, d
 /* Action -flavors*logdet + energyP + (sum (dx_t)^2/omega + omega sum x^2)/2
  * (hamilton, simulation/organic_hmc.c:67-84). */
 EPHMC_API int ephmc_hamilton(ephmc_ctx *ctx, const double *x, double logdet, double energyP, double *H);
+
+/* ------------------------------------------------------------------ static disorder (TL mode) */
+/* Transient-localisation histograms, the GPU form of hist_trans_loc
+ * (simulation/organic_trans_loc.c:25-83); run_trans_loc (:85-114) is a loop
+ * of ephmc_tl_run over batches of bond fields.  One handle per lattice and
+ * bin count.  t, kappa, mu: the couplings as run_trans_loc receives them
+ * (H = -mu + K(x), construct_hamilton with -mu); contr_mat[6]: the output of
+ * construct_contraction_mat (simulation/organic_lattice.c:48-60), required.
+ * lanes: samples processed concurrently, each lane from its own host thread
+ * (each lane holds about 7 V^2 doubles of device memory; 0 or 1 = one at a
+ * time, on the calling thread). */
+typedef struct ephmc_tl ephmc_tl;
+EPHMC_API int ephmc_tl_create(ephmc_tl **out, unsigned l1, unsigned l2, unsigned nbins, const double t[3],
+                              const double kappa[3], double mu, const double contr_mat[6], unsigned lanes,
+                              int device);
+EPHMC_API int ephmc_tl_destroy(ephmc_tl *tl);
+EPHMC_API int ephmc_tl_set_stream(ephmc_tl *tl, void *stream);
+/* The bin width of run_trans_loc, (-2 mu + 8 sum_k |kappa_k|) / nbins. */
+EPHMC_API int ephmc_tl_default_width(const ephmc_tl *tl, double *width);
+/* nsamples bond fields x[nsamples][3V] (host or device, layout [site][link],
+ * the reference's random_vector draw per sample):
+ *   hist[nbins] += sum over samples of the sample histogram (not divided by
+ *                  the number of samples; run_trans_loc divides at the end)
+ *   z[nsamples]  = the partition sums / V, results[0] of each hist_trans_loc
+ *                  call (may be NULL)
+ * hist and z may be host or device memory.  Bins at or beyond nbins are
+ * dropped (the reference writes them past the end of greens). */
+EPHMC_API int ephmc_tl_run(ephmc_tl *tl, const double *x, unsigned nsamples, double width, double *hist, double *z);
+/* Device milliseconds of the stages of the first sample that the last run
+ * gave lane 0: ms[0] Hamiltonian, [1] eigensolver, [2] current operators,
+ * [3] matrix-element products, [4] Boltzmann weights and binning.  With
+ * several lanes the stages overlap other lanes' work. */
+EPHMC_API int ephmc_tl_last_timings(const ephmc_tl *tl, float ms[5]);
 
 /* ------------------------------------------------------------------ memory */
 EPHMC_API void *ephmc_alloc(size_t bytes);   /* device memory on the current device */

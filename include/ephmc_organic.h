@@ -2,7 +2,7 @@
  * Drop-in surface of libephmc_cuda.so: the reference's own function names and
  * prototypes, so the reference's C host code (organic_main.c, organic_R.c)
  * links against this library in place of organic_dense_matrix.o,
- * organic_hmc.o and organic_bosons.o.  Each declaration cites the reference
+ * organic_hmc.o, organic_bosons.o and organic_trans_loc.o.  Each declaration cites the reference
  * prototype it replaces.
  *
  * Pointers may be host memory (as the reference's own callers pass them) or
@@ -127,6 +127,20 @@ EPHMC_API void evolve_bosons_approx_step(ephmc_dcomplex *xc, double omega, unsig
 EPHMC_API void boson_force(double *x, double *p_dot, double omega, unsigned ns, unsigned nn, unsigned nt,
                            int overwrite);                                          /* :20 */
 
+/* ---- simulation/organic_trans_loc.h:4-6 (static disorder) ---- */
+/* One sample on the GPU; greens[nt] += its histogram, results[0] = partition
+ * sum / ns, the bond field in x[0 .. 3ns).  Bins at or beyond nt are dropped
+ * (the reference writes them past the end of greens). */
+EPHMC_API void hist_trans_loc(double *x, double *t, double *kappa, double mu, double *contr_mat, unsigned *nnt,
+                              unsigned ns, unsigned nn, unsigned nt, double width, double *results, double *greens,
+                              FILE *res_out);                                       /* :4 */
+/* Seeded with time(NULL), or with the environment variable EPHMC_SEED when set;
+ * the samples' bond fields are drawn in the reference's order and the samples
+ * are diagonalised in batches, EPHMC_TL_LANES (1-16, default 4) at a time. */
+EPHMC_API unsigned run_trans_loc(double *greens, unsigned l1, unsigned l2, unsigned nt, double *t, double *kappa,
+                                 double mu, double *contr_mat, unsigned meas, const char *res_name,
+                                 const char *corr_name);                            /* :6 */
+
 /* ---- plan handles (FFTW3 argument lists, simulation/organic_hmc.c:319-322) ---- */
 EPHMC_API fftw_plan ephmc_fftw_plan_many_dft_r2c(int rank, const int *n, int howmany, double *in, const int *inembed,
                                                  int istride, int idist, ephmc_dcomplex *out, const int *onembed,
@@ -148,6 +162,10 @@ EPHMC_API unsigned ephmc_run_hmc_seeded(unsigned long long seed, double *greens,
                                         unsigned flavors, double *contr_mat, unsigned steps, double traj_length,
                                         unsigned therm, unsigned meas, unsigned meas_freq, const char *res_name,
                                         const char *corr_name, organic_flags *mode);
+/* run_trans_loc with an explicit seed instead of time(NULL) (simulation/organic_trans_loc.c:97). */
+EPHMC_API unsigned ephmc_run_trans_loc_seeded(unsigned long long seed, double *greens, unsigned l1, unsigned l2,
+                                              unsigned nt, double *t, double *kappa, double mu, double *contr_mat,
+                                              unsigned meas, const char *res_name, const char *corr_name);
 /* Force algorithm used by the drop-in force() / leap_frog (default EPHMC_FORCE_REFERENCE). */
 EPHMC_API void ephmc_set_dropin_force_mode(int force_mode);
 

@@ -273,6 +273,8 @@ class Reference(_Lib):
         s("ref_boson_force", None, [_P, _P, _D, _U, _U, _I])
         s("ref_run_main", _I, [C.c_ulong, C.c_char_p, C.c_char_p, C.c_char_p])
         s("ref_ctx_cc_correlator", None, [_P, _P, _P, _D, _P])
+        s("ref_trans_loc_samples", _I, [C.c_ulong, _U, _U, _U, _P, _P, _D, _P, _D, _U, _P, _P, _P])
+        s("ref_run_trans_loc", _U, [C.c_ulong, _U, _U, _U, _P, _P, _D, _P, _U, C.c_char_p, C.c_char_p, _P])
         self.lib.ref_init()
 
     def set_threads(self, n):
@@ -292,6 +294,30 @@ class Reference(_Lib):
         ns, nn = C.c_uint(), C.c_uint()
         self.lib.ref_lattice(l1, l2, _ptr(nnt), C.byref(ns), C.byref(nn))
         return nnt
+
+    def trans_loc_samples(self, seed, l1, l2, nbins, t, kappa, mu, contr_mat, width, nsamples):
+        """hist_trans_loc x nsamples on the stream seeded with `seed`
+        (simulation/organic_trans_loc.c:25-83, 102-103).  Returns (greens
+        summed over samples, z per sample, bond fields [nsamples][3V], whether
+        a bin past the end was written)."""
+        g = np.zeros(nbins)
+        z = np.empty(nsamples)
+        xs = np.empty((nsamples, 3 * l1 * l2))
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        t, kappa, contr_mat = f64(t), f64(kappa), f64(contr_mat)
+        ov = self.lib.ref_trans_loc_samples(seed, l1, l2, nbins, _ptr(t), _ptr(kappa), mu, _ptr(contr_mat), width,
+                                            nsamples, _ptr(g), _ptr(z), _ptr(xs))
+        return g, z, xs, bool(ov)
+
+    def run_trans_loc(self, seed, l1, l2, nbins, t, kappa, mu, contr_mat, meas, res_name, corr_name):
+        """run_trans_loc (simulation/organic_trans_loc.c:85-114), time(NULL) = seed."""
+        g = np.zeros(nbins + meas)
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        t, kappa, contr_mat = f64(t), f64(kappa), f64(contr_mat)
+        n = self.lib.ref_run_trans_loc(seed, l1, l2, nbins, _ptr(t), _ptr(kappa), mu, _ptr(contr_mat), meas,
+                                       res_name.encode() if res_name else None,
+                                       corr_name.encode() if corr_name else None, _ptr(g))
+        return g, n
 
     def context(self, m: Model):
         return RefContext(self, m)
@@ -439,3 +465,57 @@ def rel_max(a, b):
     den = np.max(np.abs(b)) if b.size else 0.0
     num = np.max(np.abs(a - b)) if a.size else 0.0
     return 0.0 if den == 0 and num == 0 else num / den
+
+
+# ---------------------------------------------------------------------- static disorder (TL mode)
+def contraction_matrix(a, b):
+    """construct_contraction_mat (simulation/organic_lattice.c:48-60), n = 3."""
+    m = np.empty(6)
+    for c in range(2):
+        m[3 * c] = a[c]
+        m[3 * c + 1] = .5 * (a[c] + b[c])
+        m[3 * c + 2] = .5 * (-a[c] + b[c])
+    return m
+
+
+def forward_neighbours(l1, l2):
+    """nnt[6i + 2k] of construct_triangular (simulation/organic_lattice.c:10-46):
+    site i = a + l1 b, link 0 right, 1 up, 2 up-left; returns [V][3]."""
+    i = np.arange(l1 * l2)
+    a, b = i % l1, i // l1
+    up = ((b + 1) % l2) * l1
+    return np.stack([b * l1 + (a + 1) % l1, up + a, up + (a + l1 - 1) % l1], axis=1)
+
+
+def trans_loc_sample(x, l1, l2, nbins, t, kappa, mu, contr_mat, width):
+    """One sample of hist_trans_loc (simulation/organic_trans_loc.c:25-83)
+    restated with dense numpy matrices, for small lattices:
+      H = -mu 1 + K(x)                 construct_hamilton (organic_dense_matrix.c:218-224)
+      I_k: w[i] += f v[n], w[n] -= f v[i]    apply_current_to_v (:226-249)
+      P_k[j, i] = psi_j . I_k psi_i; I = sum_c (sum_k mat[c,k] P_k)^2 (contr_gr_mat)
+      every pair E_j >= E_i adds (e^-E_i + e^-E_j) I / (width V) to bin
+      (unsigned)((E_j - E_i)/width + .5); bins past the end are dropped here.
+    Returns (histogram, partition sum / V)."""
+    V = l1 * l2
+    nb = forward_neighbours(l1, l2)
+    fac = np.asarray(t)[None, :] - np.asarray(kappa)[None, :] * np.asarray(x).reshape(V, 3)
+    H = np.zeros((V, V))
+    H[np.arange(V), np.arange(V)] += -mu
+    cur = np.zeros((3, V, V))
+    for k in range(3):
+        np.add.at(H, (np.arange(V), nb[:, k]), fac[:, k])
+        np.add.at(H, (nb[:, k], np.arange(V)), fac[:, k])
+        np.add.at(cur[k], (np.arange(V), nb[:, k]), fac[:, k])
+        np.add.at(cur[k], (nb[:, k], np.arange(V)), -fac[:, k])
+    ev, psi = np.linalg.eigh(H)
+    m = np.asarray(contr_mat).reshape(2, 3)
+    P = np.stack([psi.T @ cur[k] @ psi for k in range(3)])  # P[k, j, i]
+    I = sum((m[c, 0] * P[0] + m[c, 1] * P[1] + m[c, 2] * P[2]) ** 2 for c in range(2))
+    jj, ii = np.meshgrid(np.arange(V), np.arange(V), indexing="ij")
+    keep = ev[jj] >= ev[ii]
+    w = (np.exp(-ev[ii]) + np.exp(-ev[jj])) * I / (width * V)
+    bins = np.floor((ev[jj] - ev[ii]) / width + .5)
+    keep &= bins < nbins
+    hist = np.zeros(nbins)
+    np.add.at(hist, bins[keep].astype(np.int64), w[keep])
+    return hist, float(np.sum(np.exp(-ev)) / V)

@@ -374,3 +374,55 @@ void ref_ctx_cc_correlator(ref_ctx *c, const double *x_in, const double *M_inv, 
     cc_correlator(x, Mi, c->QM1P, R0t, c->w, c->t, c->kappa, c->mu, c->nnt, c->ns, c->nn, c->nt, greens, logDetM, &c->mode);
     free(x); free(Mi); free(R0t);
 }
+
+/* ------------------------------------------------------------------ static disorder (TL mode) */
+/* hist_trans_loc (simulation/organic_trans_loc.c:25-83) for nsamples samples in
+ * a row, the way run_trans_loc calls it (:102-103), on the MT19937-64 stream
+ * seeded with `seed`.  greens[nbins] += the summed sample histograms (not
+ * divided by nsamples); z[s] = results[0] of sample s; x_out[s*3ns ...] (may be
+ * NULL) = the bond field drawn for sample s.  The histogram is laid out as in
+ * organic_main (greens, then one result per sample) with room behind it for
+ * bins past the end, which the reference writes there; returns 1 if any such
+ * bin was written, else 0. */
+int ref_trans_loc_samples(unsigned long seed, unsigned l1, unsigned l2, unsigned nbins, const double *t_in,
+                          const double *kappa_in, double mu, const double *contr_in, double width,
+                          unsigned nsamples, double *greens, double *z, double *x_out) {
+    unsigned ns, nn;
+    unsigned *nnt = construct_triangular(l1, l2, &ns, &nn);
+    const unsigned nn2 = nn / 2, dim = ns * nn2, mat_dim = ns * ns;
+    const size_t slack = 64 * (size_t)nbins + 4096;
+    const size_t room = nbins + nsamples + slack;
+    double *buf = calloc(room, sizeof(double));
+    double *x = malloc((dim + 2 * mat_dim + ns + (nn2 + 1) * nn2) * sizeof(double));
+    double t[3], kappa[3], contr[6];
+    memcpy(t, t_in, sizeof t);
+    memcpy(kappa, kappa_in, sizeof kappa);
+    memcpy(contr, contr_in, sizeof contr);
+    int overflow = 0;
+    init_genrand64(seed);
+    for (unsigned s = 0; s < nsamples; s++) {
+        for (unsigned r = s; r < nsamples; r++) overflow |= buf[nbins + r] != 0;
+        hist_trans_loc(x, t, kappa, mu, contr, nnt, ns, nn, nbins, width, buf + nbins + s, buf, NULL);
+        z[s] = buf[nbins + s];
+        if (x_out) memcpy(x_out + (size_t)s * dim, x, sizeof(double) * dim);
+    }
+    for (size_t b = nbins + nsamples; b < room; b++) overflow |= buf[b] != 0;
+    for (unsigned b = 0; b < nbins; b++) greens[b] += buf[b];
+    free(buf);
+    free(x);
+    free(nnt);
+    return overflow;
+}
+
+/* run_trans_loc (simulation/organic_trans_loc.c:85-114) with time(NULL) = seed:
+ * greens[nbins + meas] as organic_main allocates it; returns its length. */
+unsigned ref_run_trans_loc(unsigned long seed, unsigned l1, unsigned l2, unsigned nbins, const double *t_in,
+                           const double *kappa_in, double mu, const double *contr_in, unsigned meas,
+                           const char *res_name, const char *corr_name, double *greens) {
+    double t[3], kappa[3], contr[6];
+    memcpy(t, t_in, sizeof t);
+    memcpy(kappa, kappa_in, sizeof kappa);
+    memcpy(contr, contr_in, sizeof contr);
+    g_seed_time = seed;
+    return run_trans_loc(greens, l1, l2, nbins, t, kappa, mu, contr, meas, res_name, corr_name);
+}

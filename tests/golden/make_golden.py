@@ -5,7 +5,7 @@ oracle/_ref/libephref.so (``make -C oracle ref``), and stores the outputs as
 small .npz files.  Run it in a checkout that has the reference sources
 (it is not run by the tests; the fixtures are committed):
 
-    python tests/golden/make_golden.py [--skip-cfg1]
+    python tests/golden/make_golden.py [--skip-cfg1] [--only trans_loc]
 
 Every evaluation is done twice, with 1 and with N OpenMP/OpenBLAS threads;
 the spread between the two (the reference's own reproducibility, which comes
@@ -174,15 +174,49 @@ def gen_fa(ref: Reference):
     save("fa_bosons.npz", **d)
 
 
+# static-disorder cases: (l1, l2, bins, beta, mu0, lambda, samples, seed); beta, mu0
+# and lambda in input.txt units, converted as organic_main does with STATIC_DISORDER
+TL_CASES = {
+    "L6x5_nb64": (6, 5, 64, 40.0, 0.0, (0.3, 0.15, 0.15), 3, 7),
+    "L8x8_nb128": (8, 8, 128, 40.0, 0.0, (0.3, 0.15, 0.15), 2, 8),
+    "L5x7_nb32_beta10": (5, 7, 32, 10.0, 0.5, (0.2, 0.1, 0.3), 3, 9),
+    # mu0 = -3: the default width does not cover the band; the reference writes
+    # bins past the end of greens (into the results behind it), the in-range
+    # bins are what both compute
+    "L6x6_nb64_mu-3": (6, 6, 64, 40.0, -3.0, (0.3, 0.15, 0.15), 2, 10),
+}
+TL_A, TL_B = (1.0, 0.0), (0.5, 0.8660254)
+
+
+def gen_trans_loc(ref: Reference):
+    from oracle import contraction_matrix, convert_params
+    d = {"unit_a": np.array(TL_A), "unit_b": np.array(TL_B)}
+    cm = contraction_matrix(TL_A, TL_B)
+    for tag, (l1, l2, nb, beta, mu0, lam, ns, seed) in TL_CASES.items():
+        t, kappa, mu, _ = convert_params(beta, nb, lam=lam, mu0=mu0, static_disorder=True)
+        width = (-2 * mu + 8 * np.abs(kappa).sum()) / nb
+        ref.set_threads(1)
+        g, z, xs, ov = ref.trans_loc_samples(seed, l1, l2, nb, t, kappa, mu, cm, width, ns)
+        d.update({f"{tag}_l1": l1, f"{tag}_l2": l2, f"{tag}_nbins": nb, f"{tag}_t": t, f"{tag}_kappa": kappa,
+                  f"{tag}_mu": mu, f"{tag}_width": width, f"{tag}_contr_mat": cm, f"{tag}_x": xs,
+                  f"{tag}_greens": g, f"{tag}_z": z, f"{tag}_overflow": ov, f"{tag}_seed": seed})
+    save("trans_loc.npz", **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-cfg1", action="store_true")
     ap.add_argument("--cfg1-seeds", type=int, default=50)
+    ap.add_argument("--only", choices=["trans_loc"], default=None)
     a = ap.parse_args()
     ref = Reference()
+    if a.only == "trans_loc":
+        gen_trans_loc(ref)
+        return
     gen_rng_lattice(ref)
     gen_fa(ref)
     gen_evals(ref)
+    gen_trans_loc(ref)
     if not a.skip_cfg1:
         gen_cfg1(ref, a.cfg1_seeds)
 

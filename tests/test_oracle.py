@@ -174,3 +174,67 @@ def test_reference_classical_acceleration_step_matches_its_formula(reference):
     xn = x.reshape(nt, ld) + np.fft.irfft((h / f2)[:, None] * np.fft.rfft(p.reshape(nt, ld), axis=0), n=nt, axis=0)
     assert np.max(np.abs(xr - xn.ravel())) <= 1e-13
     assert np.array_equal(pr, p)
+
+
+TL_CASES = ["L6x5_nb64", "L8x8_nb128", "L5x7_nb32_beta10", "L6x6_nb64_mu-3"]
+
+
+def _tl_case(g, tag):
+    return dict(l1=int(g[f"{tag}_l1"]), l2=int(g[f"{tag}_l2"]), nbins=int(g[f"{tag}_nbins"]), t=g[f"{tag}_t"],
+                kappa=g[f"{tag}_kappa"], mu=float(g[f"{tag}_mu"]), contr_mat=g[f"{tag}_contr_mat"],
+                width=float(g[f"{tag}_width"]))
+
+
+@pytest.mark.parametrize("tag", TL_CASES)
+def test_trans_loc_restatement_matches_reference_fixture(tag):
+    """The numpy restatement of hist_trans_loc against the reference's own
+    output (tests/golden/trans_loc.npz, simulation/organic_trans_loc.c:25-83)
+    on the reference's bond fields: histograms within 1e-10 of the largest bin
+    (measured 1e-13), partition sums within 1e-12."""
+    from oracle import trans_loc_sample
+    g = golden("trans_loc.npz")
+    c = _tl_case(g, tag)
+    xs = g[f"{tag}_x"]
+    h = np.zeros(c["nbins"])
+    z = []
+    for x in xs:
+        hs, zs = trans_loc_sample(x, **c)
+        h += hs
+        z.append(zs)
+    ref = g[f"{tag}_greens"]
+    assert np.max(np.abs(h - ref)) <= 1e-10 * np.max(np.abs(ref))
+    assert np.allclose(z, g[f"{tag}_z"], rtol=1e-12, atol=0)
+    # the mu0 = -3 case is the one whose default width leaves bins past the end
+    assert bool(g[f"{tag}_overflow"]) == (tag == "L6x6_nb64_mu-3")
+
+
+def test_trans_loc_reference_reproduces_its_fixture(reference):
+    """The fixture generator's call, repeated on this host: the same MT19937-64
+    bond fields bit for bit and the same histogram to 1e-12 (OpenBLAS may pick
+    other kernels on another CPU)."""
+    g = golden("trans_loc.npz")
+    tag = "L6x5_nb64"
+    c = _tl_case(g, tag)
+    reference.set_threads(1)
+    h, z, xs, ov = reference.trans_loc_samples(int(g[f"{tag}_seed"]), c["l1"], c["l2"], c["nbins"], c["t"],
+                                               c["kappa"], c["mu"], c["contr_mat"], c["width"], len(g[f"{tag}_z"]))
+    assert np.array_equal(xs, g[f"{tag}_x"])
+    assert np.max(np.abs(h - g[f"{tag}_greens"])) <= 1e-12 * np.max(np.abs(h))
+    assert np.allclose(z, g[f"{tag}_z"], rtol=1e-13, atol=0) and not ov
+
+
+def test_trans_loc_degenerate_spectrum_is_ill_posed_in_the_reference(reference):
+    """Without disorder (lambda = 0) a 4x4 lattice has exactly degenerate
+    levels.  The reference keeps pairs with E_j >= E_i, so an exactly tied
+    pair counts twice and a pair split by one ulp once: bin 0 then depends on
+    the eigensolver's rounding.  LAPACK's dsyev (the reference) and numpy's
+    eigh disagree there by up to a factor 2, while every other bin agrees.
+    Parity cases therefore carry disorder."""
+    from oracle import contraction_matrix, convert_params, trans_loc_sample
+    t, kappa, mu, _ = convert_params(10.0, 32, lam=(0, 0, 0), mu0=0.0, static_disorder=True)
+    cm = contraction_matrix((1.0, 0.0), (0.5, 0.8660254))
+    width = (-2 * mu + 8 * np.abs(kappa).sum()) / 32 * 1.0137
+    reference.set_threads(1)
+    h, _, xs, _ = reference.trans_loc_samples(7, 4, 4, 32, t, kappa, mu, cm, width, 1)
+    r, _ = trans_loc_sample(xs[0], 4, 4, 32, t, kappa, mu, cm, width)
+    assert np.max(np.abs(h[1:] - r[1:])) <= 1e-10 * np.max(np.abs(h))
