@@ -13,6 +13,12 @@ replicas (one process per GPU, no data-path collective).
 
 `--impl reference` times the reference's own C/OpenMP implementation
 (oracle/_ref, compiled unmodified) on this host's cores, rank 0 only.
+
+`--workload trans_loc` measures the static-disorder mode instead:
+disorder samples/s of hist_trans_loc (simulation/organic_trans_loc.c:25-83) on
+a 64x64 lattice (V = 4096) with 512 frequency bins, beta = 40, one step = one
+batch of `--tl-batch` samples (ephmc_tl_run); with `--impl reference` the
+reference's hist_trans_loc on the host, one sample per step.
 """
 from __future__ import annotations
 
@@ -47,6 +53,30 @@ ADJ_SWEEP_FLOP = 173 * V * V * NT
 SWEEP1_FLOP = 84 * V * V * NT
 # LU + inverse (getrf + getri): 2 V^3
 LU_FLOP = 2 * V ** 3
+
+
+# static-disorder workload: input.txt units, converted as organic_main does with
+# STATIC_DISORDER.  mu0 = 0: then run_trans_loc's default bin width spans the
+# whole band; with mu0 < 0 the reference writes bins past the end of greens.
+TL_L, TL_BINS, TL_BETA, TL_MU0 = 64, 512, 40.0, 0.0
+TL_A, TL_B = (1.0, 0.0), (0.5, 0.8660254)
+TL_METRIC = "disorder samples/s, TL mode 64x64 lattice (V=4096), 512 bins, beta=40"
+TL_UNIT = "samples/s"
+TL_WORKLOAD = "static disorder: 64x64 triangular lattice (V=4096), 512 frequency bins, beta=40, mu0=0"
+
+
+def tl_params():
+    sys.path.insert(0, os.path.join(ROOT, "electron-phonon-hmc_b200"))
+    import ephmc
+    t, kappa, mu, _ = ephmc.convert_params(TL_BETA, TL_BINS, J, LAM, TL_MU0, OMEGA0, static_disorder=True)
+    return t, kappa, mu, ephmc.contraction_matrix(TL_A, TL_B)
+
+
+def tl_flop_per_sample(V):
+    """Nominal FP64 work of one sample: tridiagonalisation 4/3 V^3, eigenvector
+    back-transformation 2 V^3, the two triangular matrix-element products
+    2 x V^3 (the tridiagonal divide and conquer is not counted)."""
+    return (4.0 / 3.0 + 2.0 + 2.0) * V ** 3
 
 
 def dist_env():
@@ -164,6 +194,164 @@ def run_reference_arm(args):
     return 0
 
 
+def run_reference_trans_loc(args):
+    """The reference's hist_trans_loc (oracle/_ref) on the host, one disorder
+    sample of the TL workload per step; at most one untimed warm-up sample and
+    a sample capped at about 5 minutes."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Reference
+    ref = Reference()
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    t, kappa, mu, cm = tl_params()
+    width = (-2 * mu + 8 * np.abs(kappa).sum()) / TL_BINS
+    times = []
+    budget = 300.0
+    t0 = time.perf_counter()
+    for k in range(max(1, args.steps)):
+        a = time.perf_counter()
+        ref.trans_loc_samples(100 + k, TL_L, TL_L, TL_BINS, t, kappa, mu, cm, width, 1)
+        times.append(time.perf_counter() - a)
+        if time.perf_counter() - t0 > budget:
+            break
+    per = sum(times) / len(times)
+    val = 1.0 / per
+    line = {"impl": "reference", "metric": TL_METRIC, "value": val, "unit": TL_UNIT, "n_gpus": ws,
+            "steps": len(times), "warmup": 0, "ms_per_step": per * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": TL_WORKLOAD, "global_batch": 1, "parallelism": "host cores"},
+            "cpu_baseline": {"value": val, "unit": TL_UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"{len(times)} disorder samples of the workload (LAPACKE dsyev on "
+                                       f"{cores} OpenBLAS threads, pair loop single-threaded as written)"},
+            "e2e": {"value": val, "unit": TL_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_trans_loc_bench(args):
+    """Disorder samples/s of the GPU path: W warm-up and K timed batches of
+    --tl-batch samples through ephmc_tl_run, bond fields resident in HBM; then
+    the same through the C ABI with host buffers (e2e)."""
+    import torch
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    import ephmc
+    lib = ephmc.load_library()
+    t, kappa, mu, cm = tl_params()
+    B = max(1, args.tl_batch)
+    W = max(3, args.warmup)
+    K = max(1, args.steps)
+    if args.profile:  # under ncu: one warm-up and one timed sample, nothing printed
+        B, W, K = 1, 1, 1
+    Lt = args.tl_l
+    V = Lt * Lt
+    tl = ephmc.TransLoc(Lt, Lt, TL_BINS, t, kappa, mu, cm, lanes=args.tl_lanes, device=local)
+    width = tl.default_width()
+    stream = torch.cuda.current_stream(dev)
+    tl.set_stream(stream.cuda_stream)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(4321 + rank)
+    xs = torch.randn((K + W) * B, 3 * V, dtype=torch.float64, device=dev, generator=gen)
+    hist = torch.zeros(TL_BINS, dtype=torch.float64, device=dev)
+    z = torch.zeros(B, dtype=torch.float64, device=dev)
+    for w in range(W):
+        tl.run(xs[(K + w) * B:(K + w + 1) * B], width, hist, z)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.ephmc_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    stages = []
+    with ClockSampler(local) as sampler:
+        for k in range(K):
+            ev[k][0].record(stream)
+            tl.run(xs[k * B:(k + 1) * B], width, hist, z)
+            ev[k][1].record(stream)
+            stages.append(tl.last_timings())
+        torch.cuda.synchronize()
+    launches = lib.ephmc_launch_count() - launches0
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), dist, dev)
+    value = ws * K * B / (total_ms / 1e3)
+    if args.profile:
+        tl.close()
+        return 0
+    # e2e: host bond fields (pinned) in, host histogram and partition sums out
+    xh = torch.empty(B, 3 * V, dtype=torch.float64, pin_memory=True)
+    xh.copy_(xs[:B].cpu())
+    hh = np.zeros(TL_BINS)
+    zh = np.zeros(B)
+    tl.set_stream(0)
+    tl.run(xh.numpy(), width, hh, zh)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(K):
+        tl.run(xh.numpy(), width, hh, zh)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    e2e = {"value": ws * K * B / e2e_s, "unit": TL_UNIT, "h2d_bytes_per_step": 8 * B * 3 * V,
+           "d2h_bytes_per_step": 8 * (TL_BINS + B)}
+    if rank == 0:
+        a = torch.randn(4096, 4096, dtype=torch.float64, device=dev)
+        for _ in range(2):
+            torch.mm(a, a)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            torch.mm(a, a)
+        e1.record()
+        torch.cuda.synchronize()
+        dgemm_tflops = 5 * 2 * 4096 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+        st = [statistics.median(s[i] for s in stages) for i in range(5)]
+        flop = tl_flop_per_sample(V)
+        ach = flop * ws * K * B / (total_ms / 1e3) / 1e12 / ws
+        prod_flop = 2.0 * V ** 3
+        # the two triangular products and the binning pass, from lane 0's stage events
+        kernels = {
+            "cusolverDnDsyevd (library)": {"ms": st[1]},
+            "cublasDsyrkx x2 (library)": {"ms": st[3], "achieved_tflops": prod_flop / (st[3] * 1e-3) / 1e12,
+                                          "peak_tflops": dgemm_tflops},
+            "k_tl_current": {"ms": st[2], "bytes": 8 * 3 * V * V,
+                             "achieved_gbs": 8 * 3 * V * V / (st[2] * 1e-3) / 1e9},
+            "k_tl_boltzmann + k_tl_bin": {"ms": st[4], "bytes": 8 * V * (V + 1),
+                                          "achieved_gbs": 8 * V * (V + 1) / (st[4] * 1e-3) / 1e9},
+            "k_tl_hamilton + memset": {"ms": st[0]}}
+        line = {"metric": TL_METRIC, "value": value, "unit": TL_UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+                "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": TL_WORKLOAD if Lt == TL_L else f"static disorder: {Lt}x{Lt} lattice (V={V}), "
+                                                                      f"512 bins, beta=40, mu0=0",
+                           "global_batch": B * ws, "samples_per_step_per_gpu": B,
+                           "lanes": args.tl_lanes, "parallelism": f"replicas x{ws}",
+                           "l2": f"inputs larger than L2 (each sample's matrices: {7 * 8 * V * V / 1e6:.0f} MB)",
+                           "inputs": "bond fields x ~ N(0,1) (torch.randn, seed 4321+rank)"},
+                "roofline": {"bound": "fp64 tensor", "kernel": "whole sample (eigensolver-dominated)",
+                             "achieved": ach, "peak": dgemm_tflops, "unit": "TFLOP/s",
+                             "frac": ach / dgemm_tflops if dgemm_tflops else None,
+                             "peak_source": "cuBLAS DGEMM 4096^3 measured in this run",
+                             "algorithmic_flop_per_sample": flop, "traffic": None,
+                             "stage_ms_lane0": dict(zip(["hamiltonian", "eigensolver", "current", "products",
+                                                         "binning"], st)),
+                             "kernels": kernels},
+                "cpu_baseline": None, "e2e": e2e, "gpu_launches": launches, "clocks": sampler.summary()}
+        print(json.dumps(line), flush=True)
+    tl.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def max_over_ranks(value, dist, device):
     """The largest of `value` over all ranks (the slowest replica sets the
     whole-job time); `value` itself when not distributed."""
@@ -201,7 +389,13 @@ def main():
     ap.add_argument("--paths", default="mixed,adjoint,reference")
     ap.add_argument("--profile", action="store_true",
                     help="run only warm-up + timed evaluations of --paths (for ncu); print nothing")
+    ap.add_argument("--workload", default="hmc", choices=["hmc", "trans_loc"])
+    ap.add_argument("--tl-batch", type=int, default=16, help="trans_loc: disorder samples per step")
+    ap.add_argument("--tl-lanes", type=int, default=2, help="trans_loc: samples diagonalised concurrently")
+    ap.add_argument("--tl-l", type=int, default=TL_L, help="trans_loc: lattice extent (profiling on smaller cases)")
     args = ap.parse_args()
+    if args.workload == "trans_loc":
+        return run_reference_trans_loc(args) if args.impl == "reference" else run_trans_loc_bench(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     W = max(3, args.warmup)

@@ -136,7 +136,7 @@ EPHMC_API void hist_trans_loc(double *x, double *t, double *kappa, double mu, do
                               FILE *res_out);                                       /* :4 */
 /* Seeded with time(NULL), or with the environment variable EPHMC_SEED when set;
  * the samples' bond fields are drawn in the reference's order and the samples
- * are diagonalised in batches, EPHMC_TL_LANES (1-16, default 4) at a time. */
+ * are diagonalised in batches, EPHMC_TL_LANES (1-16, default 2) at a time. */
 EPHMC_API unsigned run_trans_loc(double *greens, unsigned l1, unsigned l2, unsigned nt, double *t, double *kappa,
                                  double mu, double *contr_mat, unsigned meas, const char *res_name,
                                  const char *corr_name);                            /* :6 */
