@@ -43,10 +43,11 @@ def headers():
 
 
 def stale():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not all(os.path.exists(os.path.join(LIBDIR, p)) for p in PROGRAMS):
         return True
     t = os.path.getmtime(LIB)
-    return any(os.path.getmtime(f) > t for f in sources() + headers() + [__file__])
+    progs = [os.path.join(CSRC, s) for s in PROGRAMS.values()]
+    return any(os.path.getmtime(f) > t for f in sources() + headers() + progs + [__file__])
 
 
 def build(force=False, verbose=False):
@@ -78,7 +79,23 @@ def build(force=False, verbose=False):
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lcusolver", "-lcublas"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_programs(verbose)
     return LIB
+
+
+PROGRAMS = {"organic_conv": "organic_conv_main.cpp"}
+
+
+def build_programs(verbose=False):
+    """Command-line programs over the library (the reference's organic_conv
+    interface), linked with an rpath to the library's directory."""
+    for name, src in PROGRAMS.items():
+        out = os.path.join(LIBDIR, name)
+        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, os.path.join(CSRC, src), "-o", out, "-L", LIBDIR,
+               "-lephmc_cuda", "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
 
 
 if __name__ == "__main__":

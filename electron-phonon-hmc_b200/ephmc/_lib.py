@@ -92,6 +92,8 @@ def load_library(path: str | None = None, build_if_missing: bool = True):
     sig("ephmc_tl_default_width", _I, [_P, C.POINTER(_D)])
     sig("ephmc_tl_run", _I, [_P, _P, _U, _D, _P, _P])
     sig("ephmc_tl_last_timings", _I, [_P, C.POINTER(C.c_float)])
+    sig("ephmc_conv_sigma_w", _I, [_P, _U, _D, _P, _U, _P])
+    sig("ephmc_conv_sigma_t", _I, [_P, _U, _D, _P, _U, _U, _U, _P])
     sig("ephmc_alloc", _P, [C.c_size_t])
     sig("ephmc_free", None, [_P])
     sig("ephmc_device_synchronize", _I, [])

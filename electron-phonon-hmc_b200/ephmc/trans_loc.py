@@ -10,6 +10,30 @@ import numpy as np
 from ._lib import check, load_library, ptr
 
 
+def conv_sigma_w(sigma, h, widths):
+    """Smeared conductivity of organic_conv (simulation/organic_conv.c:92-111)
+    at every bin's frequency: [n][len(widths)] (ephmc_conv_sigma_w)."""
+    lib = load_library()
+    sg = np.ascontiguousarray(sigma, dtype=np.float64)
+    wd = np.ascontiguousarray(widths, dtype=np.float64)
+    out = np.empty((len(sg), len(wd)))
+    check(lib.ephmc_conv_sigma_w(sg.ctypes.data, len(sg), float(h), wd.ctypes.data, len(wd), out.ctypes.data),
+          "ephmc_conv_sigma_w")
+    return out
+
+
+def conv_sigma_t(sigma, h, widths, nt, nt_matsubara=0):
+    """Euclidean-time transform of organic_conv (:113-121) at t = i/nt,
+    i <= nt/2: [nt/2+1][len(widths)] (ephmc_conv_sigma_t)."""
+    lib = load_library()
+    sg = np.ascontiguousarray(sigma, dtype=np.float64)
+    wd = np.ascontiguousarray(widths, dtype=np.float64)
+    out = np.empty((nt // 2 + 1, len(wd)))
+    check(lib.ephmc_conv_sigma_t(sg.ctypes.data, len(sg), float(h), wd.ctypes.data, len(wd), int(nt),
+                                 int(nt_matsubara), out.ctypes.data), "ephmc_conv_sigma_t")
+    return out
+
+
 def contraction_matrix(a, b):
     """construct_contraction_mat (simulation/organic_lattice.c:48-60) for the
     triangular lattice: rows c = 0, 1 (Cartesian), columns k = right, top

@@ -18,8 +18,9 @@
  * Pointers: every double* argument of the native surface may be a device
  * pointer (used in place) or a host pointer (staged through the context's
  * device buffers, copies included in the call).  Sizes are plain unsigned.
- * No call allocates device memory after ephmc_ctx_create except
- * ephmc_ctx_create itself and the explicit ephmc_alloc.
+ * No context call allocates device memory after ephmc_ctx_create, except the
+ * explicit ephmc_alloc.  The static-disorder handle grows its per-run
+ * buffers on demand, and ephmc_conv_* allocate per call.
  *
  * Errors: every ephmc_ function returns an ephmc_status; the most recent
  * status of the calling thread, including calls made through the drop-in
@@ -238,6 +239,20 @@ EPHMC_API int ephmc_tl_run(ephmc_tl *tl, const double *x, unsigned nsamples, dou
  * [3] matrix-element products, [4] Boltzmann weights and binning.  With
  * several lanes the stages overlap other lanes' work. */
 EPHMC_API int ephmc_tl_last_timings(const ephmc_tl *tl, float ms[5]);
+
+/* ------------------------------------------------------------------ conductivity post-processing */
+/* The computations of organic_conv (simulation/organic_conv.c:9-121) on a
+ * histogram sigma[n] of bin width h (the contents of greens.bin), for n_smear
+ * smearing widths (already multiplied by beta, as organic_conv's main does):
+ *   out[i*n_smear + k] = smeared_sigma_w(i h, sigma, widths[k], h, n),  i < n
+ * and for the Euclidean-time transform, t = i / nt, i <= nt/2:
+ *   out[i*n_smear + k] = smeared_sigma_t(t, sigma, widths[k], h, n, nt_matsubara)
+ * (organic_conv's main passes nt_matsubara = 0: tanh-sinh quadrature).
+ * Pointers may be host or device memory. */
+EPHMC_API int ephmc_conv_sigma_w(const double *sigma, unsigned n, double h, const double *widths, unsigned n_smear,
+                                 double *out);
+EPHMC_API int ephmc_conv_sigma_t(const double *sigma, unsigned n, double h, const double *widths, unsigned n_smear,
+                                 unsigned nt, unsigned nt_matsubara, double *out);
 
 /* ------------------------------------------------------------------ memory */
 EPHMC_API void *ephmc_alloc(size_t bytes);   /* device memory on the current device */

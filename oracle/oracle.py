@@ -275,6 +275,9 @@ class Reference(_Lib):
         s("ref_ctx_cc_correlator", None, [_P, _P, _P, _D, _P])
         s("ref_trans_loc_samples", _I, [C.c_ulong, _U, _U, _U, _P, _P, _D, _P, _D, _U, _P, _P, _P])
         s("ref_run_trans_loc", _U, [C.c_ulong, _U, _U, _U, _P, _P, _D, _P, _U, C.c_char_p, C.c_char_p, _P])
+        s("smeared_sigma_w", _D, [_D, _P, _D, _D, _U])
+        s("smeared_sigma_t", _D, [_D, _P, _D, _D, _U, _U])
+        s("ref_run_conv", _I, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p])
         self.lib.ref_init()
 
     def set_threads(self, n):
@@ -308,6 +311,25 @@ class Reference(_Lib):
         ov = self.lib.ref_trans_loc_samples(seed, l1, l2, nbins, _ptr(t), _ptr(kappa), mu, _ptr(contr_mat), width,
                                             nsamples, _ptr(g), _ptr(z), _ptr(xs))
         return g, z, xs, bool(ov)
+
+    def conv_sigma_w(self, sigma, h, widths):
+        """smeared_sigma_w (simulation/organic_conv.c:92-111) at omega = i h for
+        every bin i and width: [n][len(widths)]."""
+        sg = np.ascontiguousarray(sigma, dtype=np.float64)
+        n = len(sg)
+        return np.array([[self.lib.smeared_sigma_w(i * h, _ptr(sg), w, h, n) for w in widths] for i in range(n)])
+
+    def conv_sigma_t(self, sigma, h, widths, nt, nt_matsubara=0):
+        """smeared_sigma_t (:113-121) at t = i / nt, i <= nt/2: [nt/2+1][len(widths)]."""
+        sg = np.ascontiguousarray(sigma, dtype=np.float64)
+        n = len(sg)
+        return np.array([[self.lib.smeared_sigma_t(i / nt, _ptr(sg), w, h, n, nt_matsubara) for w in widths]
+                         for i in range(nt // 2 + 1)])
+
+    def run_conv(self, greens, smear, out_w, out_t=None):
+        """organic_conv's main (simulation/organic_conv.c:123-164)."""
+        return self.lib.ref_run_conv(greens.encode(), smear.encode(), out_w.encode(),
+                                     out_t.encode() if out_t else None)
 
     def run_trans_loc(self, seed, l1, l2, nbins, t, kappa, mu, contr_mat, meas, res_name, corr_name):
         """run_trans_loc (simulation/organic_trans_loc.c:85-114), time(NULL) = seed."""
@@ -519,3 +541,82 @@ def trans_loc_sample(x, l1, l2, nbins, t, kappa, mu, contr_mat, width):
     hist = np.zeros(nbins)
     np.add.at(hist, bins[keep].astype(np.int64), w[keep])
     return hist, float(np.sum(np.exp(-ev)) / V)
+
+
+# ---------------------------------------------------------------------- organic_conv restated
+HALF_PI_REF = 1.570796326794897  # simulation/organic_aux.h:10
+PI_REF = 3.141592653589793
+
+
+def _tanhc(x):
+    x = np.asarray(x, dtype=np.float64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.where(x != 0, np.tanh(x) / np.where(x != 0, x, 1.0), 1.0)
+
+
+def _sigma_of_w(w, t, omega, width):
+    """sigma_of_w (simulation/organic_conv.c:9-17)."""
+    effW = -(w * width + omega)
+    tt = t * effW
+    with np.errstate(over="ignore"):
+        return np.exp(tt) / (1 + w * w) * (1 + np.exp(effW - 2 * tt)) / (1 + np.exp(effW))
+
+
+def _integral_sigma(t, omega, width):
+    """calc_integral_sigma (:19-49) for an array of omega: tanh-sinh, step
+    0.03, at most 200 nodes, each element stopping at its first term below
+    DBL_EPSILON times its running sum."""
+    omega = np.asarray(omega, dtype=np.float64)
+    if t > .5:
+        t = 1 - t
+    if t == 0:
+        return np.full(omega.shape, PI_REF)
+    h = 0.03
+    s = HALF_PI_REF * _sigma_of_w(0.0, t, omega, width)
+    active = np.ones(omega.shape, dtype=bool)
+    for i in range(1, 200):
+        x = i * h
+        sh_x = HALF_PI_REF * np.sinh(x)
+        ch_x = HALF_PI_REF * np.cosh(x)
+        w = np.sinh(sh_x)
+        val = _sigma_of_w(w, t, omega, width) + _sigma_of_w(w, t, -omega, width)
+        term = val * (ch_x * np.cosh(sh_x))
+        active &= term >= 2.220446049250313e-16 * s
+        if not active.any():
+            break
+        s = np.where(active, s + term, s)
+    return h * s
+
+
+def conv_sigma_w(sigma, h, widths):
+    """smeared_sigma_w (simulation/organic_conv.c:92-111) for every bin's
+    frequency i h and every width: [n][len(widths)]."""
+    sigma = np.asarray(sigma, dtype=np.float64)
+    n = len(sigma)
+    om = np.arange(n) * h
+    x0 = np.arange(n) * h
+    out = np.empty((n, len(widths)))
+    pre = PI_REF * .5 * _tanhc(.5 * om)
+    for k, wd in enumerate(widths):
+        if wd == 0:
+            out[:, k] = np.where(np.arange(n) == 0, sigma, pre * sigma)
+            continue
+        d1 = om[:, None] - x0[None, :]
+        d2 = om[:, None] + x0[None, :]
+        ker = wd / (PI_REF * (wd * wd + d1 * d1)) + wd / (PI_REF * (wd * wd + d2 * d2))
+        out[:, k] = pre * h * (ker @ sigma)
+    return out
+
+
+def conv_sigma_t(sigma, h, widths, nt):
+    """smeared_sigma_t (:113-121) with the tanh-sinh kernel (eval_GK_kernel
+    with nt = 0, :65-75) at t = i/nt, i <= nt/2: [nt/2+1][len(widths)]."""
+    sigma = np.asarray(sigma, dtype=np.float64)
+    om = np.arange(len(sigma)) * h
+    out = np.empty((nt // 2 + 1, len(widths)))
+    for i in range(nt // 2 + 1):
+        t = i / nt
+        for k, wd in enumerate(widths):
+            ker = _sigma_of_w(0.0, t, om, 1.0) if wd == 0 else _integral_sigma(t, om, wd) / PI_REF
+            out[i, k] = h * np.sum(sigma * ker)
+    return out

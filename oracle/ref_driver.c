@@ -426,3 +426,18 @@ unsigned ref_run_trans_loc(unsigned long seed, unsigned l1, unsigned l2, unsigne
     g_seed_time = seed;
     return run_trans_loc(greens, l1, l2, nbins, t, kappa, mu, contr, meas, res_name, corr_name);
 }
+
+/* ------------------------------------------------------------------ conductivity post-processing */
+/* organic_conv's main (simulation/organic_conv.c:123-164), renamed by the Makefile */
+int ref_conv_main(int argc, char **argv);
+
+int ref_run_conv(const char *greens, const char *smear, const char *out_w, const char *out_t) {
+    char *argv[6];
+    argv[0] = (char *)"organic_conv";
+    argv[1] = (char *)greens;
+    argv[2] = (char *)smear;
+    argv[3] = (char *)out_w;
+    argv[4] = (char *)out_t;
+    argv[5] = NULL;
+    return ref_conv_main(out_t ? 5 : 4, argv);
+}

@@ -5,7 +5,7 @@ oracle/_ref/libephref.so (``make -C oracle ref``), and stores the outputs as
 small .npz files.  Run it in a checkout that has the reference sources
 (it is not run by the tests; the fixtures are committed):
 
-    python tests/golden/make_golden.py [--skip-cfg1] [--only trans_loc]
+    python tests/golden/make_golden.py [--skip-cfg1] [--only trans_loc|conv]
 
 Every evaluation is done twice, with 1 and with N OpenMP/OpenBLAS threads;
 the spread between the two (the reference's own reproducibility, which comes
@@ -203,20 +203,47 @@ def gen_trans_loc(ref: Reference):
     save("trans_loc.npz", **d)
 
 
+def gen_conv(ref: Reference):
+    """organic_conv's smearing and time transform (simulation/organic_conv.c)
+    on two TL histograms: the 8x8 fixture case (128 bins) and a 16x16 lattice
+    with 512 bins; widths of the reference's smear.txt (beta = 40, nt = 48)."""
+    from oracle import contraction_matrix, convert_params
+    d = {}
+    g = np.load(os.path.join(HERE, "trans_loc.npz"))
+    cm = contraction_matrix(TL_A, TL_B)
+    t, kappa, mu, _ = convert_params(40.0, 512, lam=(0.3, 0.15, 0.15), mu0=0.0, static_disorder=True)
+    w512 = (-2 * mu + 8 * np.abs(kappa).sum()) / 512
+    ref.set_threads(1)
+    g512, _, _, _ = ref.trans_loc_samples(11, 16, 16, 512, t, kappa, mu, cm, w512, 2)
+    cases = {"L8x8_nb128": (g["L8x8_nb128_greens"] / 2, float(g["L8x8_nb128_width"])),
+             "L16x16_nb512": (g512 / 2, w512)}
+    beta, nt = 40.0, 48
+    widths = np.array([0, 2.7e-3, 6e-3, 1.0]) * beta
+    for tag, (sig, h) in cases.items():
+        d.update({f"{tag}_sigma": sig, f"{tag}_h": h, f"{tag}_widths": widths, f"{tag}_nt": nt,
+                  f"{tag}_w": ref.conv_sigma_w(sig, h, widths), f"{tag}_t": ref.conv_sigma_t(sig, h, widths, nt),
+                  f"{tag}_t_matsubara32": ref.conv_sigma_t(sig, h, widths, nt, 32)})
+    save("conv.npz", **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-cfg1", action="store_true")
     ap.add_argument("--cfg1-seeds", type=int, default=50)
-    ap.add_argument("--only", choices=["trans_loc"], default=None)
+    ap.add_argument("--only", choices=["trans_loc", "conv"], default=None)
     a = ap.parse_args()
     ref = Reference()
     if a.only == "trans_loc":
         gen_trans_loc(ref)
         return
+    if a.only == "conv":
+        gen_conv(ref)
+        return
     gen_rng_lattice(ref)
     gen_fa(ref)
     gen_evals(ref)
     gen_trans_loc(ref)
+    gen_conv(ref)
     if not a.skip_cfg1:
         gen_cfg1(ref, a.cfg1_seeds)
 

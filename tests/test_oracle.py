@@ -238,3 +238,16 @@ def test_trans_loc_degenerate_spectrum_is_ill_posed_in_the_reference(reference):
     h, _, xs, _ = reference.trans_loc_samples(7, 4, 4, 32, t, kappa, mu, cm, width, 1)
     r, _ = trans_loc_sample(xs[0], 4, 4, 32, t, kappa, mu, cm, width)
     assert np.max(np.abs(h[1:] - r[1:])) <= 1e-10 * np.max(np.abs(h))
+
+
+@pytest.mark.parametrize("tag", ["L8x8_nb128", "L16x16_nb512"])
+def test_conv_restatement_matches_reference_fixture(tag):
+    """organic_conv's smearing and tanh-sinh time transform restated in numpy
+    against the reference's smeared_sigma_w / smeared_sigma_t
+    (simulation/organic_conv.c:92-121, tests/golden/conv.npz): 1e-13
+    (measured 1.3e-15)."""
+    from oracle import conv_sigma_t, conv_sigma_w
+    g = golden("conv.npz")
+    sig, h, wd, nt = g[f"{tag}_sigma"], float(g[f"{tag}_h"]), g[f"{tag}_widths"], int(g[f"{tag}_nt"])
+    assert np.allclose(conv_sigma_w(sig, h, wd), g[f"{tag}_w"], rtol=1e-13, atol=0)
+    assert np.allclose(conv_sigma_t(sig, h, wd, nt), g[f"{tag}_t"], rtol=1e-13, atol=0)
