@@ -348,7 +348,10 @@ int refine_full(ephmc_ctx *c, const double *x, double *G, unsigned t) {
 // log det step of logDetM_and_inv_M_hat on c->M: single_particle takes log(trace M)
 // (simulation/organic_dense_matrix.c:550-551), otherwise the LU.
 int logdet_step(ephmc_ctx *c, double *ld, int *ipiv_host) {
-    if (c->flags.schur_form_inv) return ret(EPHMC_ERR_UNSUPPORTED, "SCHUR_FORM_INV (dgees) is not implemented");
+    if (c->flags.schur_form_inv && !c->flags.single_particle) {
+        const int rc = schur_check(&c->schur, c->M, (int)c->V, c->work, c->stream);
+        if (rc) return rc;
+    }
     if (c->flags.single_particle) {
         double *out = c->scratch + c->scratch_n - 8;
         int rc = launch_trace(c->M, (int)c->V, out, c->stream);
@@ -371,8 +374,16 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
     const ephmc_flags &f = c->flags;
     const size_t VV = (size_t)c->V * c->V;
     int rc;
-    if (f.schur_form_inv) return ret(EPHMC_ERR_UNSUPPORTED, "SCHUR_FORM_INV (dgees) is not implemented");
-    if (f.constant_force) {
+    if (f.constant_force && f.schur_form_inv) {
+        // construct_QM1P's Schur branch (:270-279): 1 - M^-1 (M_hat itself with
+        // SINGLE_PARTICLE), no slice products, no refinement
+        double *G0 = c->G;
+        rc = f.single_particle ? launch_copy(G0, Minv, VV, c->stream) : launch_one_minus(G0, Minv, (int)c->V, c->stream);
+        if (rc) return rc;
+        if ((rc = launch_contract_full(G0, c->c, c->lat, (int)c->nt, c->flavors, 1, f.single_particle,
+                                       std::exp(-logdet), c->force, c->stream)))
+            return rc;
+    } else if (f.constant_force) {
         // construct_QM1P(time = 0): Q_0 M^-1, refined at slice 0, used for every slice (:92-105, :267-309)
         double *G0 = c->G;
         if (!f.single_particle) rc = launch_copy(G0, Minv, VV, c->stream);
@@ -412,6 +423,11 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
                                                     (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
                                                     c->stream);
         if (rc) return rc;
+        // the adjoint never forms G: the clamp of organic_hmc.c:116 on the finished projection
+        if (f.schur_form_inv &&
+            (rc = launch_schur_clamp(c->force, (size_t)c->nt * c->V * 3, c->c.kappa,
+                                     c->flavors * (f.single_particle ? std::exp(-logdet) : 1.0), c->stream)))
+            return rc;
     }
     if (f.no_fourier_acc)
         return launch_boson_force(xd, c->force, c->omega, 3 * (int)c->V, (int)c->nt, false, c->stream);
@@ -481,6 +497,7 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     for (void *b : bufs)
         if (b) cudaFree(b);
     lu_free(c->lu);
+    schur_free(c->schur);
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
     cudaSetDevice(cur);
@@ -677,7 +694,6 @@ int ephmc_eval(ephmc_ctx *c, const double *x, double *p_dot, double *logdet, int
     if (!c || !x) return ret(EPHMC_ERR_ARG, "ephmc_eval");
     if (mode < EPHMC_FORCE_REFERENCE || mode > EPHMC_FORCE_MIXED) return ret(EPHMC_ERR_ARG, "force mode");
     const ephmc_flags &f = c->flags;
-    if (f.schur_form_inv) return ret(EPHMC_ERR_UNSUPPORTED, "SCHUR_FORM_INV (dgees) is not implemented");
     EPHMC_CUDA(cudaSetDevice(c->device));
     const size_t dim = (size_t)c->nt * c->V * 3;
     const double *xd = nullptr;

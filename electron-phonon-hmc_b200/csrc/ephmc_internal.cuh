@@ -62,6 +62,15 @@ int build_event_tables(const unsigned *nnt, int V, std::vector<int> &ev_src,
                        std::vector<int> &ev_fac, std::vector<int> &nbr);
 void triangular_lattice(unsigned l1, unsigned l2, unsigned *nnt);
 
+// ---------------------------------------------------------------- SCHUR_FORM_INV (schur.cu)
+struct SchurSolver;
+void schur_free(SchurSolver *s);
+// EPHMC_OK when the reference's Schur-factor regularisation does not apply to
+// M (then the Schur-form inverse is M^-1); EPHMC_ERR_UNSUPPORTED when it does
+int schur_check(SchurSolver **slot, const double *M, int V, double *scratch, cudaStream_t st);
+int launch_one_minus(double *G, const double *M, int V, cudaStream_t st);
+int launch_schur_clamp(double *force, size_t n, const double kappa[3], double f, cudaStream_t st);
+
 // ---------------------------------------------------------------- static disorder (trans_loc.cu)
 int tl_create_nnt(ephmc_tl **out, const unsigned *nnt, unsigned V, unsigned nbins, const double t[3],
                   const double kappa[3], double mu, const double contr_mat[6], unsigned lanes, int device);
@@ -230,4 +239,5 @@ struct ephmc_ctx {
     double *cc_part = nullptr;  // nt * V * 9 doubles: correlator partial sums
     double *scratch = nullptr;  // small device scratch (Fourier mode tables, reductions)
     size_t scratch_n = 0;
+    ephmc::SchurSolver *schur = nullptr;  // SCHUR_FORM_INV eigenvalue solver, created on first use
 };

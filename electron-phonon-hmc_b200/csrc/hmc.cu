@@ -89,6 +89,10 @@ double logdet_dev(ephmc_ctx *c, double *M, unsigned ns, unsigned flavors) {
         cudaMemcpy(&tr, c->scratch, sizeof(double), cudaMemcpyDeviceToHost);
         return std::log(tr);
     }
+    if (c->flags.schur_form_inv && schur_check(&c->schur, M, (int)ns, c->work, c->stream) != EPHMC_OK) {
+        std::fprintf(stderr, "ephmc logDetM_and_inv_M_hat: %s\n", ephmc_last_error_message());
+        return NAN;
+    }
     int sign = 1;
     ephmc_logdet_inverse(c, M, nullptr, &ld, &sign);
     if (sign < 0 && (flavors % 2)) std::printf("Negative determinant!\n");

@@ -421,8 +421,17 @@ void construct_QM1P(double *x, double *M_hat, double *QM1P, double *w, double *t
     (void)w;
     (void)nn;
     if (mode && mode->schur_form_inv) {
-        set_status(EPHMC_ERR_UNSUPPORTED, "SCHUR_FORM_INV (dgees) is not implemented");
-        return report("construct_QM1P");
+        // the Schur branch (:270-279): 1 - M_hat^-1, or M_hat itself with SINGLE_PARTICLE
+        const size_t VV = (size_t)ns * ns;
+        DView G(QM1P, VV), M(M_hat, VV);
+        if (!G.d || !M.d) return report("construct_QM1P");
+        if (mode->single_particle)
+            cudaMemcpy(G.d, M.d, sizeof(double) * VV, cudaMemcpyDeviceToDevice);
+        else if (launch_one_minus(G.d, M.d, (int)ns, 0) != EPHMC_OK)
+            return report("construct_QM1P");
+        cudaDeviceSynchronize();
+        G.back();
+        return;
     }
     ephmc_ctx *c = get_ctx(nnt, ns, nt, t, kappa, mu, 0.0, 1, mode);
     if (!c) return report("construct_QM1P");
@@ -499,13 +508,16 @@ void phonon_correlator(double *x, unsigned ns, unsigned, unsigned nt, double *gr
 double logDetM_and_inv_M_hat(double *M_hat, double *w, int *p, unsigned ns, unsigned flavors, organic_flags *mode) {
     (void)w;
     if (mode && mode->single_particle) return std::log(trace(M_hat, ns));
-    if (mode && mode->schur_form_inv) {
-        set_status(EPHMC_ERR_UNSUPPORTED, "SCHUR_FORM_INV (dgees) is not implemented");
-        report("logDetM_and_inv_M_hat");
-        return NAN;
-    }
     ephmc_ctx *c = lu_ctx(ns);
     if (!c) return NAN;
+    if (mode && mode->schur_form_inv) {
+        // the Schur-form inverse is M_hat^-1 unless the reference's regularisation applies (schur.cu)
+        DView Md(M_hat, (size_t)ns * ns);
+        if (!Md.d || schur_check(&c->schur, Md.d, (int)ns, c->work, c->stream) != EPHMC_OK) {
+            report("logDetM_and_inv_M_hat");
+            return NAN;
+        }
+    }
     double ld = 0;
     int sign = 1;
     std::vector<int> piv(ns);

@@ -171,6 +171,8 @@ FLAG_SETS = {
     "default": "",
     "no_fourier_acc": "NO_FOURIER_ACC\n",
     "classical_fourier_acc": "CLASSICAL_FOURIER_ACC\n4 0.5\n",
+    "schur_form_inv": "SCHUR_FORM_INV\n",
+    "constant_force": "CONSTANT_FORCE\n",
 }
 
 
@@ -179,8 +181,9 @@ def test_reference_organic_main_first_trajectories(gpu, reference, flags):
     """Two trajectories (no thermalisation, both measured) of the reference's
     organic_main.c linked to the GPU library against the reference program on
     the same MT19937-64 seed, with the default update (exact Fourier
-    acceleration), with NO_FOURIER_ACC and with CLASSICAL_FOURIER_ACC (4
-    sub-steps, mass 0.5): the results.csv and corr.csv rows agree to 1e-9;
+    acceleration), with NO_FOURIER_ACC, with CLASSICAL_FOURIER_ACC (4
+    sub-steps, mass 0.5), with SCHUR_FORM_INV and with CONSTANT_FORCE: the
+    results.csv and corr.csv rows agree to 1e-9;
     the measured difference is about 1e-12, the rounding difference between
     the two LU algorithms (LAPACK getrf/getri against Gauss-Jordan) carried
     through ten MD steps."""

@@ -1,0 +1,159 @@
+"""Flag variants of the force+logdet evaluation against the reference compiled
+unmodified, on the same phonon field: ZERO_FILLING, SINGLE_PARTICLE,
+CONSTANT_FORCE, NO_FOURIER_ACC and SCHUR_FORM_INV, alone and combined
+(simulation/organic_dense_matrix.c:251-309, :547-607, organic_hmc.c:86-134).
+
+Flags are the tuple of organic_flags' first seven fields (schur_form_inv,
+zero_filling, static_disorder, single_particle, constant_force,
+no_fourier_acc, classical_fourier_acc).  Model: 6x6, Nt = 16, beta = 5, in
+the Taylor-4 regime.  Log det within 1e-12, FP64 forces within 1e-10 of the
+largest entry (the reference's own 1- vs 8-thread spread at this size is
+2e-14).
+
+SCHUR_FORM_INV: the reference factors T + 1 of the real Schur form
+M_hat - 1 = Z T Z^T and returns Z (T + 1)^-1 Z^T, which is M_hat^-1 when its
+regularisation of T does not apply.  The regularisation applies when an
+eigenvalue of M_hat - 1 has real part below -1 or above 4.5e12.  Here it does
+not apply: the eigenvalues lie in [2e-9, 5.8].  In the cfg0 configuration
+(beta = 10, Nt = 16, outside the Taylor regime) it does apply, and the GPU
+path reports EPHMC_ERR_UNSUPPORTED."""
+import numpy as np
+import pytest
+
+GPU = pytest.mark.gpu
+
+FLAGS = {
+    "zero_filling": (0, 1, 0, 0, 0, 0, 0),
+    "single_particle": (0, 0, 0, 1, 0, 0, 0),
+    "constant_force": (0, 0, 0, 0, 1, 0, 0),
+    "constant_force+single_particle": (0, 0, 0, 1, 1, 0, 0),
+    "no_fourier_acc": (0, 0, 0, 0, 0, 1, 0),
+    "schur_form_inv": (1, 0, 0, 0, 0, 0, 0),
+    "schur_form_inv+constant_force": (1, 0, 0, 0, 1, 0, 0),
+    "schur_form_inv+single_particle": (1, 0, 0, 1, 0, 0, 0),
+}
+
+
+def _model(flags, beta=5.0, nt=16, mu0=-3.0):
+    from oracle import Model
+    return Model.physical(6, 6, nt, beta, mu0=mu0, flags=flags)
+
+
+@GPU
+@pytest.mark.parametrize("name", list(FLAGS))
+@pytest.mark.parametrize("mode", ["reference", "adjoint", "mixed"])
+def test_flag_variant_matches_reference(gpu, reference, restated, name, mode):
+    import ephmc
+    flags = FLAGS[name]
+    if flags[4] and mode != "reference":
+        pytest.skip("CONSTANT_FORCE uses one slice's G for every slice; the force algorithm does not enter")
+    if name == "zero_filling" and mode == "mixed":
+        pytest.skip("ZERO_FILLING's force is pure cancellation (see test_zero_filling_force_is_ill_posed); "
+                    "an FP32 sweep cannot resolve it")
+    m = _model(flags)
+    x = restated.random_x(7, m.dim)
+    reference.set_threads(1)
+    rc = reference.context(m)
+    ld_r, pd_r = rc.eval(x)
+    rc.close()
+    with ephmc.Context(m.l1, m.l2, m.nt, m.t, m.kappa, m.mu, m.omega, flags=flags) as ctx:
+        ld, pd = ctx.eval(x, mode=mode)
+    scale = float(np.max(np.abs(pd_r)))
+    err = float(np.max(np.abs(pd - pd_r))) / scale if scale > 0 else float(np.max(np.abs(pd)))
+    print(f"{name} {mode}: logdet {ld:.12g} (ref {ld_r:.12g}), force {err:.2e}")
+    if name == "zero_filling":
+        # the reference's own 1/2/4/8-thread spread here: 4e-8 in log det, 1.4e-6 in the force
+        assert abs(ld - ld_r) <= 1e-9 * abs(ld_r)
+        assert err <= 1e-3
+        return
+    assert abs(ld - ld_r) <= 1e-12 * max(1.0, abs(ld_r))
+    assert err <= (2e-3 if mode == "mixed" else 1e-10)
+
+
+def test_zero_filling_force_is_ill_posed(restated):
+    """Without the + 1, M = P_t Q_t and G_t = Q_t (P_t Q_t)^-1 P_t is the
+    identity for every t: the ZERO_FILLING force is what is left of the
+    refinement after cancellations of size |P_t| |Q_t| |M^-1|.  On the 6x6,
+    Nt = 16 model (cond M = 2e9) the force computed from LAPACK's inverse of
+    the reference's array is within 1.3e-6 of the force from the exact
+    (60-digit) inverse, while the equally accurate inverse from an LU of the
+    transposed array is 6e6 (relative to the largest entry) off.  So the
+    reference's force is reproducible only through the same elimination
+    order; the GPU's Gauss-Jordan follows LAPACK's pivot sequence on LAPACK's
+    view and lands at 1e-4."""
+    import mpmath
+
+    from oracle import _ptr
+    m = _model(FLAGS["zero_filling"])
+    x = restated.random_x(7, m.dim)
+    M = restated.construct_M_hat(m, x)
+    V = m.ns
+    mpmath.mp.dps = 60
+    exact = np.array((mpmath.matrix(M.tolist()) ** -1).tolist(), dtype=np.float64)
+    h = restated._model(m)
+    nb = np.array(restated.lattice(m.l1, m.l2)[:6 * V]).reshape(V, 6)[:, 0::2]
+    xc = np.ascontiguousarray(x)
+
+    def force(Minv):
+        G = np.empty((m.nt, V, V))
+        restated.lib.or_all_G(h, _ptr(xc), _ptr(np.ascontiguousarray(Minv)), _ptr(G))
+        p = np.empty((m.nt, V, 3))
+        for t in range(m.nt):
+            g = np.ascontiguousarray(G[t])
+            restated.lib.or_refine(h, _ptr(xc), _ptr(g), t)
+            for k in range(3):
+                p[t, :, k] = -m.kappa[k] * (g[np.arange(V), nb[:, k]] + g[nb[:, k], np.arange(V)])
+        return p.ravel()
+
+    fe = force(exact)
+    scale = np.max(np.abs(fe))
+    e_lapack = np.max(np.abs(force(np.linalg.inv(M)) - fe)) / scale
+    e_transposed = np.max(np.abs(force(np.linalg.inv(M.T).T) - fe)) / scale
+    restated.lib.or_model_free(h)
+    assert e_lapack < 1e-4 and e_transposed > 1e3, (e_lapack, e_transposed)
+
+
+@GPU
+def test_schur_clamp_is_active(gpu, reference, restated):
+    """A field scaled up so that some |G_ij + G_ji| exceed 2 (mu0 = 0, x six
+    times an N(0,1) draw; eigenvalues of M_hat - 1 in [-0.05, 75], so the
+    Schur regularisation does not apply): the reference's clamp of the
+    projection (organic_hmc.c:116) shapes the force, and the GPU's clamp on
+    the reference algorithm and on the adjoint force agrees.  Checked on the
+    unclamped reference force first: some projection must exceed the bound,
+    or the test would not test the clamp."""
+    import ephmc
+    flags = FLAGS["schur_form_inv"]
+    m = _model(flags, mu0=0.0)
+    m0 = _model((0,) * 7, mu0=0.0)
+    x = 6.0 * restated.random_x(9, m.dim)
+    reference.set_threads(1)
+    r0 = reference.context(m0)
+    _, pd_plain = r0.eval(x)
+    r0.close()
+    proj = np.abs(pd_plain.reshape(-1, 3) / np.asarray(m0.kappa)[None, :])
+    assert proj.max() > 2, f"no projection above 2 (max {proj.max():.3g})"
+    rc = reference.context(m)
+    ld_r, pd_r = rc.eval(x)
+    rc.close()
+    assert not np.allclose(pd_r, pd_plain), "the clamp did not change the reference force"
+    with ephmc.Context(m.l1, m.l2, m.nt, m.t, m.kappa, m.mu, m.omega, flags=flags) as ctx:
+        for mode in ("reference", "adjoint"):
+            ld, pd = ctx.eval(x, mode=mode)
+            err = float(np.max(np.abs(pd - pd_r)) / np.max(np.abs(pd_r)))
+            assert abs(ld - ld_r) <= 1e-12 * abs(ld_r) and err <= 1e-10, (mode, err)
+
+
+@GPU
+def test_schur_regularisation_regime_is_reported(gpu, restated):
+    """cfg0 (beta = 10, Nt = 16): eigenvalues of M_hat - 1 reach -5e5 and 2e22,
+    so the reference would zero small entries of its Schur factor; the GPU
+    path reports that instead of returning a different inverse."""
+    import ephmc
+    flags = FLAGS["schur_form_inv"]
+    m = _model(flags, beta=10.0)
+    x = restated.random_x(1, m.dim)
+    with ephmc.Context(m.l1, m.l2, m.nt, m.t, m.kappa, m.mu, m.omega, flags=flags) as ctx:
+        with pytest.raises(ephmc.EphmcError) as e:
+            ctx.eval(x, mode="reference")
+    assert e.value.status == 7 and "regularisation" in str(e.value)
