@@ -33,11 +33,15 @@ __device__ __forceinline__ Real stencil_at(const Real *__restrict__ v, int j, co
     return acc;
 }
 
-template <typename Real, typename QT, int S>
+// SEG: a segment of a checkpointed sweep (AdjointRange); without it the
+// kernel walks all slices from M^-1 and the range fields are not read
+template <typename Real, typename QT, int S, bool SEG>
 __global__ void __launch_bounds__(512) k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
                           const int *__restrict__ ev_fac, const int *__restrict__ nbr,
                           const QT *__restrict__ qstack, const double *__restrict__ Minv, int V, int nt,
-                          int R, double pref_scale, double *__restrict__ force) {
+                          int R, double pref_scale, double *__restrict__ force, AdjointRange rg_in) {
+    AdjointRange rg = rg_in;
+    if (!SEG) rg = AdjointRange{0, nt, nullptr, nullptr, nullptr, true};
     extern __shared__ unsigned char smem_raw[];
     Real *base = reinterpret_cast<Real *>(smem_raw);
     const size_t RV = (size_t)R * V;
@@ -63,13 +67,19 @@ __global__ void __launch_bounds__(512) k_adjoint(const double *__restrict__ x, C
         for (int k = 0; k < 3; ++k) nb[s][k] = (j < V) ? nbr[k * V + j] : 0;
     }
 
-    // y(0): row c of M^-1 (math) = column c of the inverse's array
-    for (int f = tid; f < nvec * V; f += T) {
-        const int r = f % nvec, j = f / nvec;
-        y[(size_t)r * V + j] = (Real)Minv[(size_t)j * V + c0 + r];
+    // y(t0): row c of M^-1 (math) = column c of the inverse's array, or the
+    // rows a previous segment left in rg.y_in
+    if (rg.y_in != nullptr) {
+        const Real *yi = static_cast<const Real *>(rg.y_in) + (size_t)c0 * V;
+        for (int f = tid; f < nvec * V; f += T) y[f] = yi[f];
+    } else {
+        for (int f = tid; f < nvec * V; f += T) {
+            const int r = f % nvec, j = f / nvec;
+            y[(size_t)r * V + j] = (Real)Minv[(size_t)j * V + c0 + r];
+        }
     }
 
-    for (int t = 0; t < nt; ++t) {
+    for (int t = rg.t0; t < rg.t1; ++t) {
         __syncthreads();
         const double *xs = x + (size_t)t * 3 * V;
         for (int e = tid; e < 3 * V; e += T) {
@@ -81,8 +91,12 @@ __global__ void __launch_bounds__(512) k_adjoint(const double *__restrict__ x, C
                 const int r = f / V, j = f % V;
                 q[f] = (j == c0 + r) ? (Real)1 : (Real)0;
             }
+        } else if (rg.q_top != nullptr && t == rg.t1 - 1) {
+            // the segment's last q is its checkpoint, kept in FP64
+            const double *qs = rg.q_top + (size_t)c0 * V;
+            for (int f = tid; f < nvec * V; f += T) q[f] = (Real)(QT)qs[f];
         } else {
-            const QT *qs = qstack + (size_t)t * VV + (size_t)c0 * V;
+            const QT *qs = qstack + (size_t)(t - rg.t0) * VV + (size_t)c0 * V;
             for (int f = tid; f < nvec * V; f += T) q[f] = (Real)qs[f];
         }
         __syncthreads();
@@ -178,6 +192,10 @@ __global__ void __launch_bounds__(512) k_adjoint(const double *__restrict__ x, C
         y = yn;
         yn = tmp;
     }
+    if (rg.y_out != nullptr) {
+        Real *yo = static_cast<Real *>(rg.y_out) + (size_t)c0 * V;
+        for (int f = tid; f < nvec * V; f += T) yo[f] = y[f];
+    }
 }
 
 }  // namespace
@@ -185,7 +203,7 @@ __global__ void __launch_bounds__(512) k_adjoint(const double *__restrict__ x, C
 template <typename Real, typename QT>
 int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat, const QT *qstack,
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
-                         double *force, cudaStream_t st) {
+                         double *force, cudaStream_t st, const AdjointRange *range) {
     const int V = lat.V;
     int S = 16;
     for (int o : {1, 2, 4, 8, 16})
@@ -206,28 +224,32 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     const size_t smem = per_vec * R + fac_b;
     double pref = (double)flavors;
     if (single_particle) pref *= exp(-logdet);
-    EPHMC_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * (size_t)nt * V * 3, st));
+    AdjointRange rg{0, nt, nullptr, nullptr, nullptr, true};
+    if (range) rg = *range;
+    if (rg.zero_force) EPHMC_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * (size_t)nt * V * 3, st));
     void (*kern)(const double *, Couplings, const int *, const int *, const int *, const QT *, const double *,
-                 int, int, int, double, double *) = nullptr;
+                 int, int, int, double, double *, AdjointRange) = nullptr;
+    const bool seg = range != nullptr;
     switch (S) {
-        case 1: kern = k_adjoint<Real, QT, 1>; break;
-        case 2: kern = k_adjoint<Real, QT, 2>; break;
-        case 4: kern = k_adjoint<Real, QT, 4>; break;
-        case 8: kern = k_adjoint<Real, QT, 8>; break;
-        default: kern = k_adjoint<Real, QT, 16>; break;
+        case 1: kern = seg ? k_adjoint<Real, QT, 1, true> : k_adjoint<Real, QT, 1, false>; break;
+        case 2: kern = seg ? k_adjoint<Real, QT, 2, true> : k_adjoint<Real, QT, 2, false>; break;
+        case 4: kern = seg ? k_adjoint<Real, QT, 4, true> : k_adjoint<Real, QT, 4, false>; break;
+        case 8: kern = seg ? k_adjoint<Real, QT, 8, true> : k_adjoint<Real, QT, 8, false>; break;
+        default: kern = seg ? k_adjoint<Real, QT, 16, true> : k_adjoint<Real, QT, 16, false>; break;
     }
     EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<(V + R - 1) / R, T, smem, st>>>(x, c, lat.ev_src, lat.ev_fac, lat.nbr, qstack, Minv, V, nt, R, pref,
-                                           force); ephmc::count_launch(1);
+                                           force, rg);
+    ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
     return EPHMC_OK;
 }
 
 template int launch_adjoint_sweep<double, double>(const double *, const Couplings &, const LatticeDev &,
                                                   const double *, const double *, int, unsigned, int, double,
-                                                  double *, cudaStream_t);
+                                                  double *, cudaStream_t, const AdjointRange *);
 template int launch_adjoint_sweep<float, float>(const double *, const Couplings &, const LatticeDev &,
                                                 const float *, const double *, int, unsigned, int, double,
-                                                double *, cudaStream_t);
+                                                double *, cudaStream_t, const AdjointRange *);
 
 }  // namespace ephmc

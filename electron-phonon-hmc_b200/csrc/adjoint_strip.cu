@@ -103,10 +103,16 @@ __device__ __forceinline__ float link_term(const Site8 &i, const Site8 &n, float
 
 __device__ __forceinline__ double pick3(const double (&a)[3], int k) { return k == 0 ? a[0] : k == 1 ? a[1] : a[2]; }
 
+// SEG: a segment of a checkpointed sweep (AdjointRange); without it the
+// kernel walks all slices from M^-1 and the range fields are not read
+template <bool SEG>
 __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restrict__ x, Couplings cp,
                                                           const float *__restrict__ qstack,
                                                           const double *__restrict__ Minv, int L2, int nt,
-                                                          double pref, double *__restrict__ force) {
+                                                          double pref, double *__restrict__ force,
+                                                          AdjointRange rg_in) {
+    AdjointRange rg = rg_in;
+    if (!SEG) rg = AdjointRange{0, nt, nullptr, nullptr, nullptr, true};
     extern __shared__ float sm[];
     const int V = 32 * L2, nw = L2 / kH;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -130,17 +136,23 @@ __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restri
         live[r] = cvec[r] < V;
     }
 
-    // y(0): row c of M^-1 (column c of the inverse's array)
+    // y(t0): row c of M^-1 (column c of the inverse's array), or the rows a
+    // previous segment left in rg.y_in
+    const float *y_in = static_cast<const float *>(rg.y_in);
     float y[kR][kH];
 #pragma unroll
     for (int r = 0; r < kR; ++r)
 #pragma unroll
-        for (int h = 0; h < kH; ++h)
-            y[r][h] = live[r] ? (float)Minv[(size_t)((b0 + h) * 32 + lane) * V + cvec[r]] : 0.f;
+        for (int h = 0; h < kH; ++h) {
+            const int i = (b0 + h) * 32 + lane;
+            y[r][h] = !live[r] ? 0.f
+                      : y_in  ? y_in[(size_t)cvec[r] * V + i]
+                              : (float)Minv[(size_t)i * V + cvec[r]];
+        }
     for (int e = threadIdx.x; e < 6 * V; e += blockDim.x) acc[e] = 0.f;
     __syncthreads();
 
-    for (int t = 0; t < nt; ++t) {
+    for (int t = rg.t0; t < rg.t1; ++t) {
         float *acc_t = acc + (t & 1) * 3 * V;
         const double *xs = x + (size_t)t * 3 * V;
         // FP32 hopping coefficients of the thread's sites
@@ -162,15 +174,21 @@ __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restri
                 f2p = hp[h].f2;
             }
         }
-        // q(t): the stack entry (slices 0..nt-2) or e_c (slice nt-1)
+        // q(t): the stack entry t - t0, the segment's FP64 checkpoint (its last
+        // slice, checkpointed evaluation), or e_c (slice nt-1)
         float q[kR][kH];
+        const bool top = rg.q_top != nullptr && t == rg.t1 - 1;
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
-            const float *qs = qstack + (size_t)t * VV + (size_t)cvec[r] * V;
+            const float *qs = qstack + (size_t)(t - rg.t0) * VV + (size_t)cvec[r] * V;
+            const double *qt = top ? rg.q_top + (size_t)cvec[r] * V : nullptr;
 #pragma unroll
             for (int h = 0; h < kH; ++h) {
                 const int i = (b0 + h) * 32 + lane;
-                q[r][h] = !live[r] ? 0.f : (t == nt - 1) ? (i == cvec[r] ? 1.f : 0.f) : __ldg(qs + i);
+                q[r][h] = !live[r]        ? 0.f
+                          : (t == nt - 1) ? (i == cvec[r] ? 1.f : 0.f)
+                          : top           ? (float)qt[i]
+                                          : __ldg(qs + i);
             }
         }
         float hq[kR][kH], hy[kR][kH], f0q[kR][kH], f1y[kR][kH], hf0q[kR][kH], hf1y[kR][kH];
@@ -295,6 +313,14 @@ __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restri
             acc_t[e] = 0.f;
         }
     }
+    if (rg.y_out != nullptr) {
+        float *y_out = static_cast<float *>(rg.y_out);
+#pragma unroll
+        for (int r = 0; r < kR; ++r)
+            if (live[r])
+#pragma unroll
+                for (int h = 0; h < kH; ++h) y_out[(size_t)cvec[r] * V + (b0 + h) * 32 + lane] = y[r][h];
+    }
 }
 
 }  // namespace
@@ -305,18 +331,26 @@ bool adjoint_strip_supported(const LatticeDev &lat) {
 
 int launch_adjoint_strip(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
-                         double *force, cudaStream_t st) {
+                         double *force, cudaStream_t st, const AdjointRange *range) {
     if (!adjoint_strip_supported(lat)) return EPHMC_ERR_UNSUPPORTED;
     const int V = lat.V, L2 = lat.l2, nw = L2 / kH;
     const size_t smem = sizeof(float) * (6 * (size_t)V + 2 * (size_t)kG * kSlots * kR * nw * 32);
     if (smem > 227 * 1024) return EPHMC_ERR_UNSUPPORTED;
     double pref = (double)flavors;
     if (single_particle) pref *= exp(-logdet);
-    EPHMC_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * (size_t)nt * V * 3, st));
-    EPHMC_CUDA(cudaFuncSetAttribute(k_adjoint_strip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    AdjointRange rg{0, nt, nullptr, nullptr, nullptr, true};
+    if (range) rg = *range;
+    if (rg.zero_force) EPHMC_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * (size_t)nt * V * 3, st));
     const int per_cta = kG * kR;
-    k_adjoint_strip<<<(V + per_cta - 1) / per_cta, kG * nw * 32, smem, st>>>(x, c, qstack, Minv, L2, nt, pref,
-                                                                           force);
+    if (range) {
+        EPHMC_CUDA(cudaFuncSetAttribute(k_adjoint_strip<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_adjoint_strip<true><<<(V + per_cta - 1) / per_cta, kG * nw * 32, smem, st>>>(x, c, qstack, Minv, L2, nt,
+                                                                                     pref, force, rg);
+    } else {
+        EPHMC_CUDA(cudaFuncSetAttribute(k_adjoint_strip<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_adjoint_strip<false><<<(V + per_cta - 1) / per_cta, kG * nw * 32, smem, st>>>(x, c, qstack, Minv, L2, nt,
+                                                                                      pref, force, rg);
+    }
     ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
     return EPHMC_OK;

@@ -207,8 +207,117 @@ int stage_out(ephmc_ctx *c, double *user, const double *devbuf, size_t n) {
     return EPHMC_OK;
 }
 
+// The reference algorithm's G_t for every slice and its refinement scratch:
+// allocated by the first call that needs them, so that contexts used only
+// through the adjoint paths hold O(V^2) plus the q stack (or its checkpoints).
+int ensure_ref(ephmc_ctx *c) {
+    const size_t VV = (size_t)c->V * c->V;
+    auto get = [&](double **p, size_t n) {
+        if (*p) return true;
+        if (cudaMalloc((void **)p, sizeof(double) * n) != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            return false;
+        }
+        return true;
+    };
+    if (!get(&c->G, VV * c->nt) || !get(&c->A, VV * c->refine_batch) || !get(&c->B, VV * c->refine_batch))
+        return ret(EPHMC_ERR_NOMEM, "reference-algorithm buffers (G_t for every slice, refinement scratch)");
+    return EPHMC_OK;
+}
+
+// ------------------------------------------------------------------ checkpointed adjoint
+// Segments of the sweep, from the top: b_0 = nt > b_1 = nt - C > ... > b_m = 0.
+// c->qstack holds the FP64 states Q_{b_j} = B_{b_j}...B_{nt-1}, j = 1..m-1
+// (sweep 1's rows after slice b_j), then one segment's stack of C entries.
+std::vector<int> ckpt_bounds(unsigned nt, unsigned C) {
+    std::vector<int> b{(int)nt};
+    while (b.back() > 0) b.push_back(std::max(0, b.back() - (int)C));
+    return b;
+}
+
+size_t qstack_bytes_for(unsigned nt, unsigned C, size_t VV) {
+    if (C == 0) return sizeof(double) * VV * nt;
+    const size_t m = (nt + C - 1) / C;
+    return sizeof(double) * VV * ((m - 1) + C);
+}
+
+double *ckpt_state(ephmc_ctx *c, int j) {
+    return static_cast<double *>(c->qstack) + (size_t)(j - 1) * c->V * c->V;
+}
+
+void *ckpt_segment(ephmc_ctx *c, size_t m) { return static_cast<double *>(c->qstack) + (m - 1) * c->V * c->V; }
+
+int launch_sweep1(ephmc_ctx *c, const double *x, const SliceJob *jobs_dev, bool stack_float) {
+    if (slices_strip_supported(c->lat))
+        return stack_float ? launch_slices_strip<float>(x, c->c, c->lat, jobs_dev, 1, c->stream)
+                           : launch_slices_strip<double>(x, c->c, c->lat, jobs_dev, 1, c->stream);
+    if (stack_float) return launch_slices<double, double, float>(Axis::Rows, x, c->c, c->lat, jobs_dev, 1, c->stream);
+    return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, jobs_dev, 1, c->stream);
+}
+
+// sweep 1 keeping only the checkpoints: one launch per segment, the FP64 state
+// passed through memory, so M_hat and every later recomputed q equal those of
+// the uncheckpointed sweep bit for bit
+int build_M_hat_ckpt(ephmc_ctx *c, const double *x, bool stack_float, double *dst) {
+    const std::vector<int> b = ckpt_bounds(c->nt, c->ckpt);
+    const int m = (int)b.size() - 1;
+    std::vector<SliceJob> v;
+    for (int j = 0; j < m; ++j) {
+        SliceJob jb = job(j == 0 ? nullptr : ckpt_state(c, j), j == m - 1 ? dst : ckpt_state(c, j + 1), b[j] - 1,
+                          b[j] - b[j + 1], -1, 0, kPairs, 1);
+        jb.add_identity = (j == m - 1) && !(c->flags.zero_filling || c->flags.single_particle);
+        v.push_back(jb);
+    }
+    int rc = upload_jobs(c, v, c->jobs);
+    for (int j = 0; j < m && rc == EPHMC_OK; ++j) rc = launch_sweep1(c, x, c->jobs + j, stack_float);
+    return rc;
+}
+
+// sweep 2 segment by segment, bottom up: recompute the segment's q(t) from its
+// checkpoint into the segment stack, then run the adjoint over the segment
+// with y carried between segments in c->work[2V^2, 3V^2)
+int adjoint_ckpt(ephmc_ctx *c, const double *x, const double *y0, bool mixed, double logdet) {
+    const std::vector<int> b = ckpt_bounds(c->nt, c->ckpt);
+    const int m = (int)b.size() - 1;
+    const size_t VV = (size_t)c->V * c->V;
+    void *seg = ckpt_segment(c, m);
+    double *junk = c->work + VV;       // final states of the recomputations (not needed)
+    void *ybuf = c->work + 2 * VV;     // y between segments (FP64 or FP32 rows)
+    std::vector<SliceJob> v;
+    for (int j = m - 1; j >= 0; --j) {
+        const int t0 = b[j + 1], t1 = b[j];
+        SliceJob jb = job(j == 0 ? nullptr : ckpt_state(c, j), junk, t1 - 1, t1 - t0, -1, 0, kPairs, 1);
+        jb.stack = seg;
+        jb.stack_off = -1 - t0;
+        v.push_back(jb);
+    }
+    int rc = upload_jobs(c, v, c->jobs + m);
+    const ephmc_flags &f = c->flags;
+    for (int k = 0; k < m && rc == EPHMC_OK; ++k) {
+        const int j = m - 1 - k;
+        const int t0 = b[j + 1], t1 = b[j];
+        if (t1 - t0 > 1 && (rc = launch_sweep1(c, x, c->jobs + m + k, mixed))) break;
+        AdjointRange rg{t0, t1, j == 0 ? nullptr : ckpt_state(c, j), j == m - 1 ? nullptr : ybuf,
+                        j == 0 ? nullptr : ybuf, j == m - 1};
+        if (!mixed)
+            rc = launch_adjoint_sweep<double, double>(x, c->c, c->lat, static_cast<const double *>(seg), y0,
+                                                      (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
+                                                      c->stream, &rg);
+        else if (adjoint_strip_supported(c->lat))
+            rc = launch_adjoint_strip(x, c->c, c->lat, static_cast<const float *>(seg), y0, (int)c->nt, c->flavors,
+                                      f.single_particle, logdet, c->force, c->stream, &rg);
+        else
+            rc = launch_adjoint_sweep<float, float>(x, c->c, c->lat, static_cast<const float *>(seg), y0,
+                                                    (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
+                                                    c->stream, &rg);
+    }
+    return rc;
+}
+
 // M_hat (or, with a stack, sweep 1 of the adjoint) into dst (default c->M)
 int build_M_hat(ephmc_ctx *c, const double *x, void *stack, bool stack_float, double *dst = nullptr) {
+    if (stack && c->ckpt) return build_M_hat_ckpt(c, x, stack_float, dst ? dst : c->M);
     SliceJob j = job(nullptr, dst ? dst : c->M, (int)c->nt - 1, (int)c->nt, -1, 0, kPairs, 1);
     j.add_identity = !(c->flags.zero_filling || c->flags.single_particle);
     j.stack = stack;
@@ -245,8 +354,9 @@ int all_G(ephmc_ctx *c, const double *x, const double *Minv = nullptr, double *G
           int *perm_out = nullptr) {
     const unsigned nt = c->nt;
     const size_t VV = (size_t)c->V * c->V;
-    double *G = Gbase ? Gbase : c->G;
     int rc;
+    if ((rc = ensure_ref(c))) return rc;
+    double *G = Gbase ? Gbase : c->G;
     if (!c->flags.single_particle) rc = launch_copy(G, Minv ? Minv : c->M, VV, c->stream);
     else rc = launch_identity(G, (int)c->V, c->stream);
     if (rc) return rc;
@@ -292,6 +402,7 @@ int all_G(ephmc_ctx *c, const double *x, const double *Minv = nullptr, double *G
 
 // refine_QM1P + force contraction for every slice, in batches of refine_batch slices
 int refine_all(ephmc_ctx *c, const double *x, double logdet, const double *Gbase = nullptr) {
+    if (int e = ensure_ref(c)) return e;
     const unsigned nt = c->nt;
     const size_t VV = (size_t)c->V * c->V;
     const int nb = c->refine_batch;
@@ -374,6 +485,7 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
     const ephmc_flags &f = c->flags;
     const size_t VV = (size_t)c->V * c->V;
     int rc;
+    if (f.constant_force && (rc = ensure_ref(c))) return rc;
     if (f.constant_force && f.schur_form_inv) {
         // construct_QM1P's Schur branch (:270-279): 1 - M^-1 (M_hat itself with
         // SINGLE_PARTICLE), no slice products, no refinement
@@ -411,7 +523,9 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
             if ((rc = launch_identity(c->work, (int)c->V, c->stream))) return rc;
             y0 = c->work;
         }
-        if (!mixed)
+        if (c->ckpt)
+            rc = adjoint_ckpt(c, xd, y0, mixed, logdet);
+        else if (!mixed)
             rc = launch_adjoint_sweep<double, double>(xd, c->c, c->lat, static_cast<const double *>(c->qstack), y0,
                                                       (int)c->nt, c->flavors, f.single_particle, logdet, c->force,
                                                       c->stream);
@@ -435,6 +549,8 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
 }
 
 }  // namespace
+
+int ephmc::ensure_ref_buffers(ephmc_ctx *c) { return ensure_ref(c); }
 
 
 extern "C" {
@@ -544,7 +660,7 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     const size_t VV = (size_t)V * V, dim = (size_t)nt * V * 3;
     c->refine_batch = (int)std::min<unsigned>(nt, 16);
     c->jobs_cap = (int)std::max<unsigned>(2 * nt, 2 * (unsigned)c->refine_batch) + 8;
-    c->scratch_n = fa_scratch_doubles(3 * (int)V, (int)nt) + 16;
+    c->scratch_n = fa_scratch_doubles(3 * (int)V, (int)nt) + 16 + kActionScratch;
     auto fail = [&](cudaError_t e, const char *what) {
         cuda_fail(e, what);
         cudaGetLastError();
@@ -565,9 +681,6 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     ALLOC(c->x, sizeof(double) * dim);
     ALLOC(c->force, sizeof(double) * dim);
     ALLOC(c->M, sizeof(double) * VV);
-    ALLOC(c->G, sizeof(double) * VV * nt);
-    ALLOC(c->A, sizeof(double) * VV * c->refine_batch);
-    ALLOC(c->B, sizeof(double) * VV * c->refine_batch);
     c->qstack_bytes = sizeof(double) * VV * nt;
     ALLOC(c->qstack, c->qstack_bytes);
     ALLOC(c->jobs, sizeof(SliceJob) * c->jobs_cap);
@@ -619,6 +732,41 @@ int ephmc_ctx_set_params(ephmc_ctx *c, const double t[3], const double kappa[3],
     set_couplings(c, t, kappa, mu);
     c->omega = omega;
     c->flavors = flavors;
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_set_checkpoint(ephmc_ctx *c, unsigned interval) {
+    clear_status();
+    if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_checkpoint");
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    const size_t VV = (size_t)c->V * c->V;
+    const size_t need = qstack_bytes_for(c->nt, interval, VV);
+    const size_t m = interval ? (c->nt + interval - 1) / interval : 0;
+    if (interval && 2 * m > (size_t)c->jobs_cap) return ret(EPHMC_ERR_ARG, "checkpoint interval too small for Nt");
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    if (need != c->qstack_bytes) {
+        cudaFree(c->qstack);
+        c->qstack = nullptr;
+        c->qstack_bytes = 0;
+        if (cudaMalloc(&c->qstack, need) != cudaSuccess) {
+            cudaGetLastError();
+            c->qstack = nullptr;
+            return ret(EPHMC_ERR_NOMEM, "q stack / checkpoints");
+        }
+        c->qstack_bytes = need;
+    }
+    c->ckpt = interval;
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_memory(const ephmc_ctx *c, size_t *bytes) {
+    if (!c || !bytes) return ret(EPHMC_ERR_ARG, "ephmc_ctx_memory");
+    const size_t VV = (size_t)c->V * c->V, dim = (size_t)c->nt * c->V * 3;
+    size_t b = c->qstack_bytes + sizeof(double) * (2 * dim + VV + 4 * VV + (size_t)c->nt * c->V * 9 + c->scratch_n);
+    if (c->G) b += sizeof(double) * VV * c->nt;
+    if (c->A) b += 2 * sizeof(double) * VV * c->refine_batch;
+    b += sizeof(double) * VV + sizeof(int) * ((size_t)c->V + lu_sync_words((int)c->V));  // LU panel store, pivots
+    *bytes = b;
     return EPHMC_OK;
 }
 
@@ -754,6 +902,7 @@ int ephmc_all_G(ephmc_ctx *c, const double *x, const double *M_inv, double *G_ou
     if (M_inv && !c->flags.single_particle)
         if ((rc = stage_in(c, M_inv, c->M, VV, &Mi))) return ret(rc);
     const bool dev = is_device_ptr(G_out);
+    if ((rc = ensure_ref(c))) return ret(rc);
     if ((rc = all_G(c, xd, Mi, dev ? G_out : c->G, perm_out))) return ret(rc);
     if (!dev) EPHMC_CUDA(cudaMemcpyAsync(G_out, c->G, sizeof(double) * VV * c->nt, cudaMemcpyDeviceToHost, c->stream));
     EPHMC_CUDA(cudaStreamSynchronize(c->stream));

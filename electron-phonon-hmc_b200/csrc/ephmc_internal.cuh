@@ -62,6 +62,9 @@ int build_event_tables(const unsigned *nnt, int V, std::vector<int> &ev_src,
                        std::vector<int> &ev_fac, std::vector<int> &nbr);
 void triangular_lattice(unsigned l1, unsigned l2, unsigned *nnt);
 
+// reference-algorithm buffers of a context, allocated on first use (context.cu)
+int ensure_ref_buffers(ephmc_ctx *c);
+
 // ---------------------------------------------------------------- SCHUR_FORM_INV (schur.cu)
 struct SchurSolver;
 void schur_free(SchurSolver *s);
@@ -79,6 +82,19 @@ int tl_set_params(ephmc_tl *tl, const double t[3], const double kappa[3], double
 // ---------------------------------------------------------------- slice propagation
 // One job = one V x V matrix whose vectors (rows, or columns) get a sequence
 // of slice propagators, optionally spilling the state after each slice.
+// Slices [t0, t1) of an adjoint sweep 2 (checkpointed evaluation): q for
+// slice t is stack entry t - t0, except slice t1 - 1, whose q is the FP64
+// checkpoint q_top when given (and slice nt - 1, whose q is e_c); y starts
+// from the rows of y_in (the previous segment's y_out, Real = the sweep's
+// precision) or, when y_in is null, from M^-1; y_out (optional) receives y(t1).
+struct AdjointRange {
+    int t0, t1;
+    const double *q_top;
+    const void *y_in;
+    void *y_out;
+    bool zero_force;  // clear the force first (the first segment only)
+};
+
 struct SliceJob {
     const void *src;       // input matrix; nullptr = start from the identity
     void *dst;             // output matrix (may equal src)
@@ -119,14 +135,15 @@ int launch_link_refine(const double *x, const Couplings &c, const LatticeDev &la
 template <typename Real, typename QT>
 int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat,
                          const QT *qstack, const double *Minv, int nt, unsigned flavors,
-                         int single_particle, double logdet, double *force, cudaStream_t st);
+                         int single_particle, double logdet, double *force, cudaStream_t st,
+                         const AdjointRange *range = nullptr);
 
 // FP32 adjoint sweep 2 for L1 = 32 lattices with the lattice in registers
 // (adjoint_strip.cu)
 bool adjoint_strip_supported(const LatticeDev &lat);
 int launch_adjoint_strip(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
-                         double *force, cudaStream_t st);
+                         double *force, cudaStream_t st, const AdjointRange *range = nullptr);
 
 // ---------------------------------------------------------------- drop-in helpers (helpers.cu)
 // out = (mu + K) in on nvec rows (or columns) of V x V matrices, reference order;
@@ -193,6 +210,7 @@ int lu_logdet_inverse_async(double *M, LUWork &w, cudaStream_t st);
 
 // ---------------------------------------------------------------- Fourier acceleration
 // scratch: device doubles, at least fa_scratch_doubles(ld, nt)
+constexpr size_t kActionScratch = 2 * 64 + 8;  // k_action partial sums (fa_api.cu), after the FA tables
 size_t fa_scratch_doubles(int ld, int nt);
 int fa_evolve(double *x, double *p, int ld, int nt, double omega, double h, double *scratch, cudaStream_t st);
 int fa_scale_modes(double *v, int ld, int nt, double omega, int mode, double *scratch, cudaStream_t st);
@@ -220,12 +238,13 @@ struct ephmc_ctx {
     double *x = nullptr;      // nt*V*3
     double *force = nullptr;  // nt*V*3
     double *M = nullptr;      // V*V  (M_hat, then its inverse)
-    double *G = nullptr;      // nt*V*V (reference algorithm)
-    double *A = nullptr;      // nb*V*V refine scratch
-    double *B = nullptr;      // nb*V*V refine scratch
+    double *G = nullptr;      // nt*V*V (reference algorithm), allocated on first use
+    double *A = nullptr;      // nb*V*V refine scratch, allocated on first use
+    double *B = nullptr;      // nb*V*V refine scratch, allocated on first use
     int refine_batch = 0;
-    void *qstack = nullptr;   // (nt)*V*V (adjoint), FP64 or FP32
+    void *qstack = nullptr;   // (nt)*V*V (adjoint), FP64 or FP32; checkpoints + one segment when ckpt > 0
     size_t qstack_bytes = 0;
+    unsigned ckpt = 0;        // adjoint checkpoint interval in slices (0: whole stack)
     ephmc::SliceJob *jobs = nullptr;  // device job array
     int jobs_cap = 0;
     std::vector<ephmc::SliceJob> jobs_host;

@@ -182,7 +182,7 @@ int ephmc_hamilton(ephmc_ctx *c, const double *x, double logdet, double energyP,
         xd = c->x;
     }
     const int nblk = 64;
-    double *part = c->A;  // V*V doubles >= 2*nblk + 2
+    double *part = c->scratch + (c->scratch_n - 8 - ephmc::kActionScratch);  // 2*nblk + 2 doubles
     k_action<<<nblk, 256, 0, c->stream>>>(xd, ld, (int)c->nt, part); ephmc::count_launch(1);
     k_action_final<<<1, 32, 0, c->stream>>>(part, nblk, part + 2 * nblk); ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());

@@ -81,6 +81,16 @@ ephmc_ctx *ctx_for(unsigned *nnt, unsigned ns, unsigned nt, double *t, double *k
     return c;
 }
 
+// nt V^2 doubles for the correlator's R_0t chain: the q stack when it holds the
+// whole sweep, else the reference-algorithm G buffer (allocated on first use),
+// else `fallback`
+double *correlator_chain(ephmc_ctx *c, double *fallback) {
+    const size_t need = sizeof(double) * (size_t)c->nt * c->V * c->V;
+    if (c->qstack && c->qstack_bytes >= need) return static_cast<double *>(c->qstack);
+    if (ensure_ref_buffers(c) == EPHMC_OK) return c->G;
+    return fallback;
+}
+
 double logdet_dev(ephmc_ctx *c, double *M, unsigned ns, unsigned flavors) {
     double ld = 0;
     if (c->flags.single_particle) {
@@ -203,7 +213,7 @@ short trajectory_dev(ephmc_ctx *c, double *xb, double *results, double *greens, 
         if (greens) {
             double *gd = nullptr;
             cudaMalloc(&gd, sizeof(double) * nt * 9);
-            cc_correlator_dev(c, x, M_hat, QM1P, c->qstack ? static_cast<double *>(c->qstack) : QM1P, gd, logDetM);
+            cc_correlator_dev(c, x, M_hat, QM1P, correlator_chain(c, QM1P), gd, logDetM);
             cudaMemcpy(greens, gd, sizeof(double) * nt * 9, cudaMemcpyDeviceToHost);
             cudaFree(gd);
             if (corr_out) {  // fprint_corr (simulation/organic_aux.c:51-60)
@@ -297,8 +307,8 @@ void cc_correlator(double *x, double *M_hat, double *R_t0, double *R_0t, double 
     if (!c) return;
     const size_t dim = (size_t)nt * ns * 3, VV = (size_t)ns * ns;
     Dev X(x, dim), Mi(M_hat, VV), Rt(R_t0, VV * nt, false), G(greens, (size_t)nt * 9, false);
-    double *chain = static_cast<double *>(c->qstack);  // nt V^2 doubles
-    if (cc_correlator_dev(c, X.d, Mi.d, Rt.d, chain, G.d, logDetM) != EPHMC_OK) {
+    double *chain = correlator_chain(c, nullptr);  // nt V^2 doubles
+    if (!chain || cc_correlator_dev(c, X.d, Mi.d, Rt.d, chain, G.d, logDetM) != EPHMC_OK) {
         std::fprintf(stderr, "ephmc cc_correlator: %s\n", ephmc_last_error_message());
         return;
     }

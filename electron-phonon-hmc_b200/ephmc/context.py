@@ -139,6 +139,16 @@ class Context:
     def warnings(self):
         return self.lib.ephmc_last_warnings()
 
+    def set_checkpoint(self, interval):
+        """Checkpointed adjoint sweeps every `interval` slices (0: whole stack)."""
+        check(self.lib.ephmc_ctx_set_checkpoint(self.h, int(interval)), "ephmc_ctx_set_checkpoint")
+
+    def memory(self):
+        """Device bytes the context holds."""
+        b = C.c_size_t(0)
+        check(self.lib.ephmc_ctx_memory(self.h, C.byref(b)), "ephmc_ctx_memory")
+        return b.value
+
     # ------------------------------------------------------------ phonon side
     def fa_evolve(self, x, p, h):
         check(self.lib.ephmc_fa_evolve(self.h, ptr(x), ptr(p), float(h)), "ephmc_fa_evolve")

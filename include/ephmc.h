@@ -19,7 +19,8 @@
  * pointer (used in place) or a host pointer (staged through the context's
  * device buffers, copies included in the call).  Sizes are plain unsigned.
  * No context call allocates device memory after ephmc_ctx_create, except the
- * explicit ephmc_alloc.  The static-disorder handle grows its per-run
+ * explicit ephmc_alloc, ephmc_ctx_set_checkpoint, and the first call of the
+ * reference algorithm (its Nt V^2 G_t buffers).  The static-disorder handle grows its per-run
  * buffers on demand, and ephmc_conv_* allocate per call.
  *
  * Errors: every ephmc_ function returns an ephmc_status; the most recent
@@ -162,6 +163,22 @@ EPHMC_API int ephmc_ctx_create_nnt(ephmc_ctx **out, const unsigned *nnt, unsigne
                          const double t[3], const double kappa[3], double mu, double omega,
                          unsigned flavors, const ephmc_flags *flags, int device);
 EPHMC_API int ephmc_ctx_set_flags(ephmc_ctx *ctx, const ephmc_flags *flags);
+
+/* No counterpart in the reference.  Checkpointed adjoint sweeps: sweep 1
+ * keeps the FP64 propagator states Q_t = B_t...B_{Nt-1} only every
+ * `interval` slices, and sweep 2 recomputes each segment's states from its
+ * checkpoint before using them, so the adjoint and mixed forces hold
+ * ceil(Nt/interval) - 1 + interval matrices of V^2 doubles instead of Nt
+ * (interval ~ sqrt(Nt) minimises it).  The force, log det and M_hat are
+ * those of the whole-stack sweep (recomputation repeats the same arithmetic;
+ * only the order of the force's atomic sums differs).  One extra propagation
+ * of the V vectors through Nt - ceil(Nt/interval) slices per evaluation.
+ * interval 0 restores the whole stack.  The reference algorithm's G_t
+ * buffers (Nt V^2 doubles) are separate and allocated on first use. */
+EPHMC_API int ephmc_ctx_set_checkpoint(ephmc_ctx *ctx, unsigned interval);
+/* Device bytes the context holds now (buffers allocated on first use included
+ * once they exist). */
+EPHMC_API int ephmc_ctx_memory(const ephmc_ctx *ctx, size_t *bytes);
 
 /* force() given the inverse (simulation/organic_hmc.c:86-134): p_dot from x and
  * M_inv (the output of logDetM_and_inv_M_hat); flags as the reference
