@@ -14,6 +14,10 @@ replicas (one process per GPU, no data-path collective).
 `--impl reference` times the reference's own C/OpenMP implementation
 (oracle/_ref, compiled unmodified) on this host's cores, rank 0 only.
 
+`--workload batch` measures 64 independent chains of uneven lattice, Nt, beta
+and coupling evaluated together (ephmc_batch_eval), against the same chains
+one at a time.
+
 `--workload trans_loc` measures the static-disorder mode instead:
 disorder samples/s of hist_trans_loc (simulation/organic_trans_loc.c:25-83) on
 a 64x64 lattice (V = 4096) with 512 frequency bins, beta = 40, one step = one
@@ -77,6 +81,167 @@ def tl_flop_per_sample(V):
     back-transformation 2 V^3, the two triangular matrix-element products
     2 x V^3 (the tridiagonal divide and conquer is not counted)."""
     return (4.0 / 3.0 + 2.0 + 2.0) * V ** 3
+
+
+# batched chains: 64 independent chains of uneven lattice, Nt, beta and coupling
+BATCH_N, BATCH_SEED = 64, 2024
+BATCH_METRIC = "chain force+logdet evals/s, 64 uneven chains (L 8-32, Nt 16-64, beta 5-40) in one batch"
+BATCH_UNIT = "chain evals/s"
+
+
+def batch_chains():
+    """The 64 chains: L in {8,12,16,24,32} (square), Nt in {16,32,64},
+    beta ~ U[5,40], lambda scaled by U[0.5,1.5]; seeded.  Returns
+    (L, Nt, beta, lambda-scale) tuples."""
+    rng = np.random.default_rng(BATCH_SEED)
+    out = []
+    for _ in range(BATCH_N):
+        out.append((int(rng.choice([8, 12, 16, 24, 32])), int(rng.choice([16, 32, 64])), float(rng.uniform(5, 40)),
+                    float(rng.uniform(0.5, 1.5))))
+    return out
+
+
+def batch_flop(chains):
+    return sum((L * L) ** 2 * nt * (84 * (1 + np.log2(nt)) + 170) + 2 * (L * L) ** 3 for L, nt, _, _ in chains)
+
+
+def run_batch_bench(args):
+    """chain evals/s of the 64-chain mix: W warm-up and K timed batches of one
+    mixed-precision evaluation per chain through ephmc_batch_eval (fields
+    resident in HBM), the same chains one at a time through ephmc_eval for
+    comparison, and the batch through the C ABI with host buffers (e2e)."""
+    import torch
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    import ephmc
+    lib = ephmc.load_library()
+    chains = batch_chains()
+    W, K = max(3, args.warmup), max(1, args.steps)
+    ctxs, xs, pds = [], [], []
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(77 + rank)
+    for L, nt, beta, s in chains:
+        t, kappa, mu, omega = ephmc.convert_params(beta, nt, J, tuple(s * v for v in LAM), MU0, OMEGA0)
+        c = ephmc.Context(L, L, nt, t, kappa, mu, omega, device=local)
+        ctxs.append(c)
+        xs.append(torch.randn(c.dim, dtype=torch.float64, device=dev, generator=gen))
+        pds.append(torch.empty(c.dim, dtype=torch.float64, device=dev))
+
+    def run_batch(x, p):
+        try:
+            ephmc.batch_eval(ctxs, x, p, mode="mixed")
+        except ephmc.EphmcError as e:  # chains outside the Taylor regime may give a non-finite log det
+            if e.status != 5:
+                raise
+
+    def run_seq():
+        for c, x, p in zip(ctxs, xs, pds):
+            try:
+                c.eval(x, p, mode="mixed")
+            except ephmc.EphmcError as e:
+                if e.status != 5:
+                    raise
+
+    for _ in range(W):
+        run_batch(xs, pds)
+    run_seq()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches0 = lib.ephmc_launch_count()
+    with ClockSampler(local) as sampler:
+        t0 = time.perf_counter()
+        for _ in range(K):
+            run_batch(xs, pds)
+        torch.cuda.synchronize()
+        batch_s = time.perf_counter() - t0
+    launches = lib.ephmc_launch_count() - launches0
+    t0 = time.perf_counter()
+    for _ in range(K):
+        run_seq()
+    torch.cuda.synchronize()
+    seq_s = time.perf_counter() - t0
+    batch_s = max_over_ranks(batch_s, dist, dev)
+    seq_s = max_over_ranks(seq_s, dist, dev)
+    n = len(ctxs)
+    value = ws * K * n / batch_s
+    # e2e: host fields and forces (pinned) through the C ABI
+    xh = [torch.empty(c.dim, dtype=torch.float64, pin_memory=True) for c in ctxs]
+    ph = [torch.empty(c.dim, dtype=torch.float64, pin_memory=True) for c in ctxs]
+    for a, b in zip(xh, xs):
+        a.copy_(b.cpu())
+    xnp, pnp = [a.numpy() for a in xh], [a.numpy() for a in ph]
+    run_batch(xnp, pnp)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        run_batch(xnp, pnp)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    nbytes = sum(8 * c.dim for c in ctxs)
+    e2e = {"value": ws * K * n / e2e_s, "unit": BATCH_UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+    if rank == 0:
+        fp64 = C_float_peak(lib, True)
+        flop = batch_flop(chains)
+        ach = flop * K / batch_s / 1e12
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = batch_cpu_baseline(chains)
+            except Exception as e:
+                cpu = {"value": None, "unit": BATCH_UNIT, "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"unavailable: {e}"}
+        line = {"metric": BATCH_METRIC, "value": value, "unit": BATCH_UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+                "ms_per_step": batch_s / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64+f32", "data": "synthetic",
+                "config": {"workload": f"{n} chains, L in {{8,12,16,24,32}}, Nt in {{16,32,64}}, beta ~ U[5,40], "
+                                       f"lambda x U[0.5,1.5] (seed {BATCH_SEED}); one mixed evaluation per chain "
+                                       "per step", "global_batch": n * ws, "parallelism": f"replicas x{ws}",
+                           "l2": "fields of all chains resident; no flush (a step touches the 64 contexts' "
+                                 "buffers, several GB)"},
+                "one_chain_at_a_time": {"value": ws * K * n / seq_s, "ms_per_step": seq_s / K * 1e3},
+                "roofline": {"bound": "fp64", "kernel": "whole batch (sweeps + LU of all chains)", "achieved": ach,
+                             "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64 if fp64 else None,
+                             "peak_source": "measured in this run (CUDA-core FP64 FMA probe)",
+                             "algorithmic_flop_per_step": flop, "traffic": None},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": sampler.summary()}
+        print(json.dumps(line), flush=True)
+    for c in ctxs:
+        c.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def batch_cpu_baseline(chains, budget=60.0):
+    """The reference (oracle/_ref) on the host: one evaluation of each chain in
+    turn until all are done or `budget` seconds have passed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Model, Reference
+    ref = Reference()
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    done, spent = 0, 0.0
+    for i, (L, nt, beta, s) in enumerate(chains):
+        m = Model.physical(L, L, nt, beta, J, tuple(s * v for v in LAM), MU0, OMEGA0)
+        ctx = ref.context(m)
+        ctx.eval(ref.random_x(1 + i, m.dim))
+        spent += ctx.last_time()
+        ctx.close()
+        done += 1
+        if spent > budget:
+            break
+    return {"value": done / spent, "unit": BATCH_UNIT, "cores": cores, "kind": "reference",
+            "sample": f"one evaluation of each of the first {done} of the {len(chains)} chains, reference C "
+                      f"sources + OpenBLAS, OMP/OpenBLAS threads={cores}"}
 
 
 def dist_env():
@@ -389,13 +554,27 @@ def main():
     ap.add_argument("--paths", default="mixed,adjoint,reference")
     ap.add_argument("--profile", action="store_true",
                     help="run only warm-up + timed evaluations of --paths (for ncu); print nothing")
-    ap.add_argument("--workload", default="hmc", choices=["hmc", "trans_loc"])
+    ap.add_argument("--workload", default="hmc", choices=["hmc", "trans_loc", "batch"])
     ap.add_argument("--tl-batch", type=int, default=16, help="trans_loc: disorder samples per step")
     ap.add_argument("--tl-lanes", type=int, default=2, help="trans_loc: samples diagonalised concurrently")
     ap.add_argument("--tl-l", type=int, default=TL_L, help="trans_loc: lattice extent (profiling on smaller cases)")
     args = ap.parse_args()
     if args.workload == "trans_loc":
         return run_reference_trans_loc(args) if args.impl == "reference" else run_trans_loc_bench(args)
+    if args.workload == "batch":
+        if args.impl == "reference":
+            ws, rank, _ = dist_env()
+            if rank != 0:
+                return 0
+            cpu = batch_cpu_baseline(batch_chains(), budget=240.0)
+            print(json.dumps({"impl": "reference", "metric": BATCH_METRIC, "value": cpu["value"], "unit": BATCH_UNIT,
+                              "n_gpus": ws, "steps": 1, "warmup": 0, "ms_per_step": BATCH_N / cpu["value"] * 1e3,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                              "data": "synthetic", "config": {"workload": "the 64-chain mix", "parallelism": "host cores"},
+                              "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": BATCH_UNIT,
+                                                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+            return 0
+        return run_batch_bench(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     W = max(3, args.warmup)

@@ -614,6 +614,9 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
         if (b) cudaFree(b);
     lu_free(c->lu);
     schur_free(c->schur);
+    if (c->batch_stream) cudaStreamDestroy(c->batch_stream);
+    for (cudaEvent_t e : c->batch_ev)
+        if (e) cudaEventDestroy(e);
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
     cudaSetDevice(cur);
@@ -866,6 +869,126 @@ int ephmc_eval(ephmc_ctx *c, const double *x, double *p_dot, double *logdet, int
     if (logdet) *logdet = ld;
     if (!std::isfinite(ld)) return ret(EPHMC_ERR_NONFINITE, "log det not finite");
     return EPHMC_OK;
+}
+
+// Several chains' evaluations at once: every phase is issued for all chains
+// (each on its context's stream) before the next, and nothing waits on the
+// host until all forces are issued.  SINGLE_PARTICLE and SCHUR_FORM_INV
+// chains, whose force needs the log det or a host-side eigenvalue check
+// first, run through ephmc_eval after the others are issued.
+int ephmc_batch_eval(ephmc_ctx *const *ctxs, const double *const *x, double *const *p_dot, double *logdet,
+                     unsigned n, int mode) {
+    clear_status();
+    if (!ctxs || !x || n == 0) return ret(EPHMC_ERR_ARG, "ephmc_batch_eval");
+    if (mode < EPHMC_FORCE_REFERENCE || mode > EPHMC_FORCE_MIXED) return ret(EPHMC_ERR_ARG, "force mode");
+    for (unsigned i = 0; i < n; ++i) {
+        if (!ctxs[i] || !x[i]) return ret(EPHMC_ERR_ARG, "ephmc_batch_eval: null context or field");
+        for (unsigned j = 0; j < i; ++j)
+            if (ctxs[j] == ctxs[i]) return ret(EPHMC_ERR_ARG, "ephmc_batch_eval: a context appears twice");
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    auto sync_fast = [&](const ephmc_ctx *c) { return !c->flags.single_particle && !c->flags.schur_form_inv; };
+    // contexts on the legacy default stream run on their own stream for the
+    // batch, ordered after the work already queued on the legacy stream
+    std::vector<cudaStream_t> caller(n);
+    for (unsigned i = 0; i < n; ++i) {
+        ephmc_ctx *c = ctxs[i];
+        caller[i] = c->stream;
+        if (c->stream != nullptr || !sync_fast(c)) continue;
+        if (cudaSetDevice(c->device) != cudaSuccess) return ret(EPHMC_ERR_CUDA, "cudaSetDevice");
+        if (!c->batch_stream) {
+            if (cudaStreamCreateWithFlags(&c->batch_stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->batch_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->batch_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return ret(EPHMC_ERR_CUDA, "ephmc_batch_eval: stream creation");
+            }
+        }
+        cudaEventRecord(c->batch_ev[0], nullptr);
+        cudaStreamWaitEvent(c->batch_stream, c->batch_ev[0], 0);
+        c->stream = c->batch_stream;
+    }
+    std::vector<const double *> xd(n, nullptr);
+    int rc = EPHMC_OK;
+    unsigned issued = 0;
+    // sweep 1 (M_hat and, for the adjoint paths, the q stack or its checkpoints)
+    for (unsigned i = 0; i < n && rc == EPHMC_OK; ++i, issued = i) {
+        ephmc_ctx *c = ctxs[i];
+        if (!sync_fast(c)) continue;
+        if (cudaSetDevice(c->device) != cudaSuccess) { rc = ret(EPHMC_ERR_CUDA, "cudaSetDevice"); break; }
+        const size_t dim = (size_t)c->nt * c->V * 3;
+        const bool adj = mode != EPHMC_FORCE_REFERENCE && !c->flags.constant_force;
+        if ((rc = stage_in(c, x[i], c->x, dim, &xd[i]))) break;
+        rc = build_M_hat(c, xd[i], adj ? c->qstack : nullptr, mode == EPHMC_FORCE_MIXED);
+    }
+    // LU, inverse and log det, left on the device
+    for (unsigned i = 0; i < issued && rc == EPHMC_OK; ++i) {
+        ephmc_ctx *c = ctxs[i];
+        if (!sync_fast(c)) continue;
+        cudaSetDevice(c->device);
+        rc = lu_logdet_inverse_async(c->M, c->lu, c->stream);
+    }
+    // forces
+    for (unsigned i = 0; i < issued && rc == EPHMC_OK; ++i) {
+        ephmc_ctx *c = ctxs[i];
+        if (!sync_fast(c)) continue;
+        cudaSetDevice(c->device);
+        const bool adj = mode != EPHMC_FORCE_REFERENCE && !c->flags.constant_force;
+        if ((rc = force_core(c, xd[i], c->M, 0.0, mode, adj))) break;
+    }
+    // collect: log det, sign, status of every issued chain
+    for (unsigned i = 0; i < issued; ++i) {
+        ephmc_ctx *c = ctxs[i];
+        if (!sync_fast(c)) continue;
+        cudaSetDevice(c->device);
+        // (a copy to pageable host memory returns only when done: issued after every chain's force)
+        if (rc == EPHMC_OK && p_dot && p_dot[i]) rc = stage_out(c, p_dot[i], c->force, (size_t)c->nt * c->V * 3);
+        int info[2] = {0, 0};
+        double ld[2] = {0, 1};
+        cudaMemcpyAsync(info, c->lu.info, sizeof(info), cudaMemcpyDeviceToHost, c->stream);
+        cudaMemcpyAsync(ld, c->lu.diag + c->V, sizeof(ld), cudaMemcpyDeviceToHost, c->stream);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess && rc == EPHMC_OK)
+            rc = ret(EPHMC_ERR_CUDA, "ephmc_batch_eval: stream synchronisation");
+        if (rc != EPHMC_OK) continue;
+        if (info[1] != 0) {
+            cudaMemsetAsync(c->lu.sync, 0, sizeof(unsigned) * lu_sync_words((int)c->V), c->stream);
+            cudaStreamSynchronize(c->stream);
+            rc = ret(EPHMC_ERR_TIMEOUT, "LU: a panel wait of the dataflow kernel ran out; the result is invalid");
+            continue;
+        }
+        if (info[0] != 0) {
+            rc = ret(EPHMC_ERR_SINGULAR, "zero pivot");
+            continue;
+        }
+        c->last_logdet = ld[0];
+        c->last_sign = ld[1] < 0 ? -1 : 1;
+        c->have_inverse = true;
+        if (c->last_sign < 0 && (c->flavors % 2)) add_warning(EPHMC_WARN_NEGATIVE_DET);
+        if (logdet) logdet[i] = ld[0];
+        if (!std::isfinite(ld[0])) rc = ret(EPHMC_ERR_NONFINITE, "log det not finite");
+    }
+    // back to the callers' streams (the legacy stream waits for the batch streams)
+    for (unsigned i = 0; i < n; ++i) {
+        ephmc_ctx *c = ctxs[i];
+        if (c->stream == caller[i]) continue;
+        cudaSetDevice(c->device);
+        cudaEventRecord(c->batch_ev[1], c->stream);
+        cudaStreamWaitEvent(caller[i], c->batch_ev[1], 0);
+        c->stream = caller[i];
+    }
+    // chains whose force needs the log det first
+    for (unsigned i = 0; i < n && rc == EPHMC_OK; ++i) {
+        ephmc_ctx *c = ctxs[i];
+        if (sync_fast(c)) continue;
+        const unsigned warn = last_warnings();
+        double ld = 0;
+        rc = ephmc_eval(c, x[i], p_dot ? p_dot[i] : nullptr, &ld, mode);
+        add_warning(warn);
+        if (logdet) logdet[i] = ld;
+    }
+    cudaSetDevice(cur);
+    return rc;
 }
 
 // force() given the inverse M_inv (simulation/organic_hmc.c:86-134)

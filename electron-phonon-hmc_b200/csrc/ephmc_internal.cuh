@@ -259,4 +259,8 @@ struct ephmc_ctx {
     double *scratch = nullptr;  // small device scratch (Fourier mode tables, reductions)
     size_t scratch_n = 0;
     ephmc::SchurSolver *schur = nullptr;  // SCHUR_FORM_INV eigenvalue solver, created on first use
+    // ephmc_batch_eval: the context's own non-blocking stream, used in place of
+    // the legacy default stream so that chains overlap; created on first use
+    cudaStream_t batch_stream = nullptr;
+    cudaEvent_t batch_ev[2] = {nullptr, nullptr};
 };

@@ -7,8 +7,8 @@ the computation is the library's CUDA kernels.
 """
 from ._lib import (FORCE_ADJOINT, FORCE_MIXED, FORCE_REFERENCE, MODES, EphmcError, Flags, load_library,
                    LIB_PATH)
-from .context import Context, convert_params, lattice
+from .context import Context, batch_eval, convert_params, lattice
 from .trans_loc import TransLoc, contraction_matrix, conv_sigma_t, conv_sigma_w
 
-__all__ = ["Context", "TransLoc", "contraction_matrix", "conv_sigma_w", "conv_sigma_t", "convert_params", "lattice", "load_library", "EphmcError", "Flags", "FORCE_REFERENCE",
+__all__ = ["Context", "batch_eval", "TransLoc", "contraction_matrix", "conv_sigma_w", "conv_sigma_t", "convert_params", "lattice", "load_library", "EphmcError", "Flags", "FORCE_REFERENCE",
            "FORCE_ADJOINT", "FORCE_MIXED", "MODES", "LIB_PATH"]

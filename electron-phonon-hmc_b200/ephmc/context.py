@@ -172,3 +172,22 @@ class Context:
         H = C.c_double(0.0)
         check(self.lib.ephmc_hamilton(self.h, ptr(x), float(logdet), float(energyP), C.byref(H)), "ephmc_hamilton")
         return H.value
+
+
+def batch_eval(contexts, xs, p_dots=None, mode="mixed"):
+    """ephmc_batch_eval: one force+logdet evaluation of every chain (context
+    i on field xs[i]), all chains issued before any host wait.  xs and
+    p_dots: numpy arrays or CUDA tensors; p_dots defaults to new host arrays
+    for host fields (None entries for device fields).  Returns (logdets,
+    p_dots)."""
+    lib = load_library()
+    n = len(contexts)
+    m = MODES[mode] if isinstance(mode, str) else int(mode)
+    if p_dots is None:
+        p_dots = [np.empty(c.dim) if isinstance(x, np.ndarray) else None for c, x in zip(contexts, xs)]
+    hs = (C.c_void_p * n)(*[c.h.value if isinstance(c.h, C.c_void_p) else c.h for c in contexts])
+    xp = (C.c_void_p * n)(*[ptr(x) for x in xs])
+    pp = (C.c_void_p * n)(*[ptr(p) if p is not None else None for p in p_dots])
+    ld = (C.c_double * n)()
+    check(lib.ephmc_batch_eval(hs, xp, pp, ld, n, m), "ephmc_batch_eval")
+    return np.array(ld[:]), p_dots

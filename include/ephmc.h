@@ -127,6 +127,15 @@ EPHMC_API int ephmc_ctx_set_stream(ephmc_ctx *ctx, void *stream);
  * The inverse M_hat^-1 stays in the context (ephmc_ctx_get_inverse). */
 EPHMC_API int ephmc_eval(ephmc_ctx *ctx, const double *x, double *p_dot, double *logdet, int force_mode);
 
+/* No counterpart in the reference.  ephmc_eval for n independent chains (one
+ * context each, any lattice, Nt and couplings): the phases of all chains are
+ * issued on their contexts' streams before any host wait, so small chains
+ * overlap on the GPU.  x[i], p_dot[i]: as ephmc_eval (p_dot or p_dot[i] may
+ * be NULL); logdet[n] (host, may be NULL).  Returns the first failure; the
+ * other chains' outputs are valid. */
+EPHMC_API int ephmc_batch_eval(ephmc_ctx *const *ctxs, const double *const *x, double *const *p_dot,
+                               double *logdet, unsigned n, int force_mode);
+
 /* M_hat = 1 + B_0...B_{Nt-1} only (construct_M_hat), out[V*V] row layout of the reference. */
 EPHMC_API int ephmc_construct_M_hat(ephmc_ctx *ctx, const double *x, double *M_hat_out);
 
