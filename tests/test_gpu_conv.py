@@ -90,3 +90,17 @@ def test_organic_conv_program_against_reference_program(gpu, reference):
     assert a.shape == b.shape == (512, 5) and at.shape == bt.shape == (25, 5)
     assert np.allclose(b, a, rtol=1e-5, atol=1e-300)
     assert np.allclose(bt, at, rtol=1e-5, atol=1e-300)
+
+
+def test_conv_unsmeared_width_only(gpu):
+    """Width 0 alone (the histogram read back bin by bin, organic_conv.c:97-101)
+    and the t = 1/2 end point, against the restatement."""
+    import ephmc
+    from oracle import conv_sigma_t, conv_sigma_w
+    g = golden("conv.npz")
+    sig, h = g["L8x8_nb128_sigma"], float(g["L8x8_nb128_h"])
+    w = ephmc.conv_sigma_w(sig, h, [0.0])
+    assert np.allclose(w, conv_sigma_w(sig, h, [0.0]), rtol=1e-13, atol=0)
+    t = ephmc.conv_sigma_t(sig, h, [0.0, 5.0], 2)
+    r = conv_sigma_t(sig, h, [0.0, 5.0], 2)
+    assert t.shape == (2, 2) and np.allclose(t, r, rtol=1e-12, atol=0)

@@ -176,3 +176,27 @@ def test_reference_organic_main_static_disorder(gpu, reference):
     assert np.allclose(zg, zr, rtol=1e-12, atol=0)
     assert (ng, wg) == (nr, wr) == (64, wr)
     assert _rel(hg, hr) <= 1e-10
+
+
+def test_tl_many_bins_and_odd_lattice(gpu):
+    """Histograms past the shared-memory limit (12 000 bins: the binning
+    kernel's global-atomic variant) and a 7x5 lattice with 5 samples on 3
+    lanes, against the numpy restatement."""
+    import ephmc
+    from oracle import contraction_matrix, convert_params, trans_loc_sample
+    cm = contraction_matrix((1.0, 0.0), (0.5, 0.8660254))
+    rng = np.random.default_rng(21)
+    for (l1, l2, nbins, lanes, ns) in ((6, 6, 12000, 1, 2), (7, 5, 48, 3, 5)):
+        t, kappa, mu, _ = convert_params(20.0, nbins, mu0=0.0, static_disorder=True)
+        xs = rng.standard_normal((ns, 3 * l1 * l2))
+        with ephmc.TransLoc(l1, l2, nbins, t, kappa, mu, cm, lanes=lanes) as tl:
+            w = tl.default_width()
+            h, z = tl.run(xs, w)
+        ref = np.zeros(nbins)
+        zr = []
+        for x in xs:
+            hs, zs = trans_loc_sample(x, l1, l2, nbins, t, kappa, mu, cm, w)
+            ref += hs
+            zr.append(zs)
+        assert _rel(h, ref) <= 1e-10, (l1, l2, nbins, _rel(h, ref))
+        assert np.allclose(z, zr, rtol=1e-12, atol=0)
