@@ -45,6 +45,7 @@ UNIT = "evals/s"
 L, NT, BETA = 32, 64, 20.0
 J, LAM, MU0, OMEGA0 = (1.0, -0.5, -0.5), (0.3, 0.15, 0.15), -3.0, 0.05
 WORKLOAD = "32x32 triangular lattice (V=1024), Nt=64, beta=20, force+logdet eval"
+TRAJ_BETA = 10.0  # the timed trajectory (beta = 20 diverges in the MD, in the reference as well)
 
 # Algorithmic work of one evaluation (reference algorithm, Taylor-4 as two pairs):
 # FLOP = V^2 Nt (84 (1 + log2 Nt) + 170) + 2 V^3 ; per slice application 84 V^2 flop.
@@ -665,6 +666,37 @@ def main():
     e2e = {"value": whole_job_rate(ws, K, e2e_s), "unit": UNIT, "h2d_bytes_per_step": 8 * dim,
            "d2h_bytes_per_step": 8 * dim + 8}
 
+    # one HMC trajectory's device work: Nmd = 20 leapfrog steps with Fourier
+    # acceleration over traj_length = pi/2 (ephmc_leapfrog), then the accept
+    # step's evaluation, from a free-phonon field (run_hmc's start,
+    # simulation/organic_hmc.c:325) and accelerated momenta.  At beta = 20 the
+    # molecular dynamics diverges within two steps, in the reference's own HMC
+    # as here (acceptance 0, e^-dH NaN on 8x8, Nt = 64); the trajectory is timed
+    # on the same lattice and Nt at beta = 10, where it accepts.
+    tt, tk, tmu, tom = ephmc.convert_params(TRAJ_BETA, NT, J, LAM, MU0, OMEGA0)
+    tctx = ephmc.Context(L, L, NT, tt, tk, tmu, tom, device=local)
+    lib.ephmc_ctx_set_stream(tctx.h, stream.cuda_stream)
+    xt = torch.randn(dim, dtype=torch.float64, device=dev, generator=gen)
+    tctx.fa_scale_free_bosons(xt)
+    traj_ms, traj_fail = [], None
+    for k in range(5):
+        pt = torch.randn(dim, dtype=torch.float64, device=dev, generator=gen)
+        tctx.fa_scale_momenta(pt)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        try:
+            tctx.leapfrog(xt, pt, 20, float(np.pi / 2), head)
+            tctx.eval(xt, pd, mode=head)
+        except ephmc.EphmcError as e:
+            traj_fail = str(e)
+            break
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if k >= 2:
+            traj_ms.append(e0.elapsed_time(e1))
+    tctx.close()
+    traj = max_over_ranks(statistics.median(traj_ms), dist, dev) if traj_ms else None
+
     line = None
     if rank == 0:
         fp32 = C_float_peak(lib, False)
@@ -713,7 +745,12 @@ def main():
                           for p, v in results.items()},
                 "mixed_over_fp64_plain": (results["mixed"]["value"] / results["reference"]["value"])
                 if ("mixed" in results and "reference" in results) else None,
-                "trajectories_per_s_estimate": r["value"] / 22.0,
+                "trajectory": {"ms": traj, "trajectories_per_s": (ws * 1e3 / traj) if traj else None,
+                               "beta": TRAJ_BETA, "failed": traj_fail,
+                               "what": "device work of one trajectory at 32x32, Nt=64, beta=10: 20 leapfrog steps "
+                                       "with Fourier acceleration (ephmc_leapfrog, traj_length pi/2) + the "
+                                       "accept-step evaluation; the host momentum draw and the Metropolis scalars "
+                                       "are not included. At beta=20 the MD diverges, in the reference too"},
                 "roofline": roofline, "fp64_fma_peak_tflops": fp64, "fp32_fma_peak_tflops": fp32,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": results[head]["launches"],
                 "clocks": results[head]["clocks"]}

@@ -16,6 +16,9 @@
 // with the reference's formulas and passed in.
 #include "ephmc_internal.cuh"
 
+#include <map>
+#include <mutex>
+
 #include <cmath>
 #include <vector>
 
@@ -179,13 +182,29 @@ double freq2(double omega, int k, int n) {
 }
 
 // host mode table -> device scratch (pageable copy: the source is consumed before return)
+// what each scratch buffer's table region holds (upload cache, see fa_forget_tables)
+std::mutex g_tab_mu;
+std::map<const double *, std::vector<double>> g_tab;
+
 int upload_modes(const std::vector<double> &h, double *scratch, cudaStream_t st, double **out) {
-    EPHMC_CUDA(cudaMemcpyAsync(scratch, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
     *out = scratch;
+    {
+        std::lock_guard<std::mutex> l(g_tab_mu);
+        auto it = g_tab.find(scratch);
+        if (it != g_tab.end() && it->second == h) return EPHMC_OK;
+    }
+    if (int e = upload_small(scratch, h.data(), sizeof(double) * h.size(), st)) return e;
+    std::lock_guard<std::mutex> l(g_tab_mu);
+    g_tab[scratch] = h;
     return EPHMC_OK;
 }
 
 }  // namespace
+
+void fa_forget_tables(const double *scratch) {
+    std::lock_guard<std::mutex> l(g_tab_mu);
+    g_tab.erase(scratch);
+}
 
 int fa_evolve(double *x, double *p, int ld, int n, double omega, double h, double *scratch, cudaStream_t st) {
     if (n < 1 || n > 512) return EPHMC_ERR_UNSUPPORTED;
@@ -254,7 +273,7 @@ int fa_energy(const double *p, int ld, int n, double omega, double *out_dev, dou
     if (n < 1 || n > 512) return EPHMC_ERR_UNSUPPORTED;
     const int nc = n / 2 + 1, center = (n + 1) / 2;
     const int nblk = (ld + kTile - 1) / kTile;
-    std::vector<double> tab(nc + nblk);
+    std::vector<double> tab(nc);  // the per-CTA partials follow at d + nc (written, not accumulated)
     for (int k = 0; k < nc; ++k) {
         double w = .5 / n / freq2(omega, k, n);
         if (k > 0 && k < center) w *= 2;

@@ -166,8 +166,7 @@ int ensure_jobs(ephmc_ctx *c, int n) {
 
 int upload_jobs(ephmc_ctx *c, const std::vector<SliceJob> &jobs, SliceJob *dst) {
     if (jobs.empty()) return EPHMC_OK;
-    EPHMC_CUDA(cudaMemcpyAsync(dst, jobs.data(), sizeof(SliceJob) * jobs.size(), cudaMemcpyHostToDevice, c->stream));
-    return EPHMC_OK;
+    return ctx_upload_jobs(c, jobs.data(), (int)jobs.size(), (int)(dst - c->jobs), c->stream);
 }
 
 SliceJob job(const void *src, void *dst, int s_first, int s_count, int s_dir, int pb, int pe, int ps) {
@@ -552,6 +551,49 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
 
 int ephmc::ensure_ref_buffers(ephmc_ctx *c) { return ensure_ref(c); }
 
+// One evaluation issued on the context stream without a host wait: sweep 1,
+// LU (log det, sign and status stay in c->lu), force into c->force.  For the
+// flags whose force needs no host-side log det (not SINGLE_PARTICLE, not
+// SCHUR_FORM_INV).  xd: device field.
+int ephmc::eval_async(ephmc_ctx *c, const double *xd, int mode) {
+    if (c->flags.single_particle || c->flags.schur_form_inv)
+        return ret(EPHMC_ERR_UNSUPPORTED, "eval_async: the force needs the log det on the host");
+    const bool adj = mode != EPHMC_FORCE_REFERENCE && !c->flags.constant_force;
+    int rc;
+    if ((rc = build_M_hat(c, xd, adj ? c->qstack : nullptr, mode == EPHMC_FORCE_MIXED))) return rc;
+    if ((rc = lu_logdet_inverse_async(c->M, c->lu, c->stream))) return rc;
+    return force_core(c, xd, c->M, 0.0, mode, adj);
+}
+
+static bool same_job(const SliceJob &a, const SliceJob &b) {
+    return a.src == b.src && a.dst == b.dst && a.stack == b.stack && a.stack_off == b.stack_off &&
+           a.s_first == b.s_first && a.s_count == b.s_count && a.s_dir == b.s_dir && a.p_begin == b.p_begin &&
+           a.p_end == b.p_end && a.p_step == b.p_step && a.add_identity == b.add_identity;
+}
+
+int ephmc::ctx_upload_jobs(ephmc_ctx *c, const SliceJob *jobs, int n, int slot, cudaStream_t st) {
+    if (n <= 0) return EPHMC_OK;
+    if (slot < 0 || slot + n > c->jobs_cap) return ret(EPHMC_ERR_ARG, "job table too small");
+    if ((int)c->jobs_host.size() < c->jobs_cap) {
+        c->jobs_host.resize(c->jobs_cap);
+        c->jobs_valid.assign(c->jobs_cap, 0);
+    }
+    bool same = true;
+    for (int i = 0; i < n && same; ++i) same = c->jobs_valid[slot + i] && same_job(c->jobs_host[slot + i], jobs[i]);
+    if (same) return EPHMC_OK;
+    if (int e = upload_small(c->jobs + slot, jobs, sizeof(SliceJob) * n, st)) return e;
+    for (int i = 0; i < n; ++i) {
+        c->jobs_host[slot + i] = jobs[i];
+        c->jobs_valid[slot + i] = 1;
+    }
+    return EPHMC_OK;
+}
+
+void ephmc::ctx_forget_uploads(ephmc_ctx *c) {
+    std::fill(c->jobs_valid.begin(), c->jobs_valid.end(), 0);
+    fa_forget_tables(c->scratch);
+}
+
 
 extern "C" {
 
@@ -612,6 +654,8 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
                     c->lat.nbr,   c->lat.rev,      c->scratch,    c->work,     c->cc_part};
     for (void *b : bufs)
         if (b) cudaFree(b);
+    fa_forget_tables(c->scratch);
+    cudaFree(c->md_log);
     lu_free(c->lu);
     schur_free(c->schur);
     if (c->batch_stream) cudaStreamDestroy(c->batch_stream);
@@ -787,6 +831,7 @@ int ephmc_ctx_lattice(const ephmc_ctx *c, unsigned *nnt_out) {
 
 int ephmc_ctx_set_stream(ephmc_ctx *c, void *stream) {
     if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_stream");
+    if (c->stream != static_cast<cudaStream_t>(stream)) ctx_forget_uploads(c);  // uploads queued on the old stream
     c->stream = static_cast<cudaStream_t>(stream);
     return EPHMC_OK;
 }

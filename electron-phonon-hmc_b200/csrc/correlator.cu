@@ -111,7 +111,7 @@ int cc_correlator_dev(ephmc_ctx *c, const double *x, const double *Minv, double 
     j2.s_count = nt - 1;
     j2.s_dir = 1;
     SliceJob jobs[2] = {j1, j2};
-    EPHMC_CUDA(cudaMemcpyAsync(c->jobs, jobs, sizeof(jobs), cudaMemcpyHostToDevice, st));
+    if ((rc = ctx_upload_jobs(c, jobs, 2, 0, st))) return rc;
     if ((rc = launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs, 1, st))) return rc;
     if (nt > 1)
         if ((rc = launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs + 1, 1, st))) return rc;

@@ -64,6 +64,15 @@ void triangular_lattice(unsigned l1, unsigned l2, unsigned *nnt);
 
 // reference-algorithm buffers of a context, allocated on first use (context.cu)
 int ensure_ref_buffers(ephmc_ctx *c);
+// n slice jobs into the context's device job table at `slot`, on stream st.
+// Entries the table already holds are not copied again: a copy from pageable
+// host memory first waits for the stream to drain, so repeated evaluations
+// would otherwise stall the host once per upload.
+struct SliceJob;
+int ctx_upload_jobs(ephmc_ctx *c, const SliceJob *jobs, int n, int slot, cudaStream_t st);
+void ctx_forget_uploads(ephmc_ctx *c);
+// sweep 1 + LU + force on the context stream, no host wait (context.cu)
+int eval_async(ephmc_ctx *c, const double *xd, int mode);
 
 // ---------------------------------------------------------------- SCHUR_FORM_INV (schur.cu)
 struct SchurSolver;
@@ -166,6 +175,10 @@ int launch_add_diag(double *M, int V, double v, cudaStream_t st);
 int launch_contract_full(const double *D, const Couplings &c, const LatticeDev &lat, int nt, unsigned flavors,
                          int schur, int sp, double spw, double *force, cudaStream_t st);
 int launch_axpy(double *y, const double *x, double a, size_t n, cudaStream_t st);
+// host bytes -> device, carried in kernel parameters (captured at launch), so
+// the source may be a temporary and the stream may still be busy: a
+// cudaMemcpyAsync from pageable memory can read its source after returning
+int upload_small(void *dst, const void *src, size_t bytes, cudaStream_t st);
 int launch_pair_combine(double *v, const double *w, const double *z, double al, double aq, size_t n, cudaStream_t st);
 
 // ---------------------------------------------------------------- drop-in glue (organic_api.cu)
@@ -209,6 +222,11 @@ int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv
 int lu_logdet_inverse_async(double *M, LUWork &w, cudaStream_t st);
 
 // ---------------------------------------------------------------- Fourier acceleration
+// Mode tables of the Fourier-acceleration kernels are uploaded to the start of
+// a scratch buffer; an upload whose contents the buffer already holds is
+// skipped.  fa_forget_tables drops that knowledge (buffer freed, or its
+// stream changed).
+void fa_forget_tables(const double *scratch);
 // scratch: device doubles, at least fa_scratch_doubles(ld, nt)
 constexpr size_t kActionScratch = 2 * 64 + 8;  // k_action partial sums (fa_api.cu), after the FA tables
 size_t fa_scratch_doubles(int ld, int nt);
@@ -247,7 +265,8 @@ struct ephmc_ctx {
     unsigned ckpt = 0;        // adjoint checkpoint interval in slices (0: whole stack)
     ephmc::SliceJob *jobs = nullptr;  // device job array
     int jobs_cap = 0;
-    std::vector<ephmc::SliceJob> jobs_host;
+    std::vector<ephmc::SliceJob> jobs_host;  // what the device job table holds (upload cache)
+    std::vector<char> jobs_valid;
     ephmc::LUWork lu{};
     double last_logdet = 0;
     int last_sign = 1;
@@ -256,6 +275,8 @@ struct ephmc_ctx {
     float t_mhat = 0, t_lu = 0, t_force = 0;
     double *work = nullptr;     // 4 V*V doubles: full-matrix refinement and drop-in staging
     double *cc_part = nullptr;  // nt * V * 9 doubles: correlator partial sums
+    double *md_log = nullptr;   // ephmc_leapfrog: per MD step log det, sign, LU status (3 doubles each)
+    unsigned md_cap = 0;        // steps md_log holds
     double *scratch = nullptr;  // small device scratch (Fourier mode tables, reductions)
     size_t scratch_n = 0;
     ephmc::SchurSolver *schur = nullptr;  // SCHUR_FORM_INV eigenvalue solver, created on first use

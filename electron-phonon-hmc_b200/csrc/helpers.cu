@@ -3,6 +3,9 @@
 // operator, dense helpers and the phonon-side reductions.
 #include "ephmc_internal.cuh"
 
+#include <algorithm>
+#include <cstring>
+
 namespace ephmc {
 
 namespace {
@@ -331,6 +334,30 @@ int launch_pair_combine(double *v, const double *w, const double *z, double al, 
     k_pair_combine<<<(unsigned)std::min<size_t>((n + 255) / 256, 1184), 256, 0, st>>>(v, w, z, al, aq, n);
     count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
+    return EPHMC_OK;
+}
+
+namespace {
+constexpr int kParamBytes = 3968;  // payload of one launch, inside the 4 KB kernel-parameter space
+struct ParamChunk {
+    unsigned char b[kParamBytes];
+};
+__global__ void k_write_bytes(unsigned char *__restrict__ dst, ParamChunk c, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = c.b[i];
+}
+}  // namespace
+
+int upload_small(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+    const unsigned char *s = static_cast<const unsigned char *>(src);
+    unsigned char *d = static_cast<unsigned char *>(dst);
+    for (size_t off = 0; off < bytes; off += kParamBytes) {
+        const int n = (int)std::min<size_t>(kParamBytes, bytes - off);
+        ParamChunk c;
+        std::memcpy(c.b, s + off, n);
+        k_write_bytes<<<1, 256, 0, st>>>(d + off, c, n);
+        count_launch(1);
+        EPHMC_CUDA(cudaGetLastError());
+    }
     return EPHMC_OK;
 }
 

@@ -143,11 +143,30 @@ void update_x_dev(ephmc_ctx *c, double *x, double *p, double *p_dot, size_t dim,
     }
 }
 
+// update_x (simulation/organic_hmc.c:136-165) issued without a host wait
+int update_x_async(ephmc_ctx *c, double *x, double *p, double *p_dot, size_t dim, double h, double half) {
+    if (c->flags.classical_fourier_acc && !c->flags.no_fourier_acc) return classical_update_x(c, x, p, p_dot, h, half);
+    if (c->flags.no_fourier_acc) return launch_axpy(x, p, h * std::fabs(half), dim, c->stream);
+    return fa_evolve(x, p, 3 * (int)c->V, (int)c->nt, c->omega, std::fabs(half) * h, c->scratch, c->stream);
+}
+
+bool leapfrog_async_ok(const ephmc_ctx *c) { return !c->flags.single_particle && !c->flags.schur_form_inv; }
+
 // leap_frog (simulation/organic_hmc.c:167-190) on device buffers; M_hat ends
 // holding the inverse of the last step
 void leap_frog_dev(ephmc_ctx *c, double *x, double *p, double *p_dot, double *M_hat, unsigned steps,
                    double traj_length, int force_mode) {
     const size_t dim = (size_t)c->nt * c->V * 3, VV = (size_t)c->V * c->V;
+    if (leapfrog_async_ok(c)) {
+        unsigned neg = 0;
+        if (ephmc_leapfrog(c, x, p, steps, traj_length, force_mode, &neg) != EPHMC_OK)
+            std::fprintf(stderr, "ephmc leap_frog: %s\n", ephmc_last_error_message());
+        for (unsigned s = 0; s < neg; ++s) std::printf("Negative determinant!\n");
+        cudaMemcpyAsync(p_dot, c->force, sizeof(double) * dim, cudaMemcpyDeviceToDevice, c->stream);
+        cudaMemcpyAsync(M_hat, c->M, sizeof(double) * VV, cudaMemcpyDeviceToDevice, c->stream);
+        cudaStreamSynchronize(c->stream);
+        return;
+    }
     const double h = steps ? traj_length / steps : 2 * traj_length;
     double half = .5;
     update_x_dev(c, x, p, p_dot, dim, h, half);
@@ -258,6 +277,87 @@ short trajectory_dev(ephmc_ctx *c, double *xb, double *results, double *greens, 
 }  // namespace
 
 extern "C" {
+
+// leap_frog (simulation/organic_hmc.c:167-190) on device x and p with every
+// step issued before any host wait: per step sweep 1 + LU + force, p += h F,
+// update_x.  The log det, sign and LU status of each step stay on the device
+// and are read once at the end.
+int ephmc_leapfrog(ephmc_ctx *c, double *x, double *p, unsigned steps, double traj_length, int force_mode,
+                   unsigned *negative_steps) {
+    clear_status();
+    if (!c || !x || !p) {
+        set_status(EPHMC_ERR_ARG, "ephmc_leapfrog arguments");
+        return EPHMC_ERR_ARG;
+    }
+    if (force_mode < EPHMC_FORCE_REFERENCE || force_mode > EPHMC_FORCE_MIXED) {
+        set_status(EPHMC_ERR_ARG, "force mode");
+        return EPHMC_ERR_ARG;
+    }
+    if (!leapfrog_async_ok(c)) {
+        set_status(EPHMC_ERR_UNSUPPORTED,
+                   "ephmc_leapfrog: SINGLE_PARTICLE and SCHUR_FORM_INV forces need each step's log det on the host");
+        return EPHMC_ERR_UNSUPPORTED;
+    }
+    EPHMC_CUDA(cudaSetDevice(c->device));
+    if (!devp(x) || !devp(p)) {
+        set_status(EPHMC_ERR_ARG, "ephmc_leapfrog: x and p must be device memory");
+        return EPHMC_ERR_ARG;
+    }
+    if (steps > c->md_cap) {
+        cudaFree(c->md_log);
+        c->md_log = nullptr;
+        c->md_cap = 0;
+        if (cudaMalloc(&c->md_log, sizeof(double) * 3 * steps) != cudaSuccess) {
+            cudaGetLastError();
+            set_status(EPHMC_ERR_NOMEM, "ephmc_leapfrog: step log");
+            return EPHMC_ERR_NOMEM;
+        }
+        c->md_cap = steps;
+    }
+    const size_t dim = (size_t)c->nt * c->V * 3;
+    const double h = steps ? traj_length / steps : 2 * traj_length;
+    int rc = update_x_async(c, x, p, c->force, dim, h, .5);
+    for (unsigned s = 1; s <= steps && rc == EPHMC_OK; ++s) {
+        if ((rc = eval_async(c, x, force_mode))) break;
+        double *lg = c->md_log + 3 * (size_t)(s - 1);
+        cudaMemcpyAsync(lg, c->lu.diag + c->V, 2 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+        cudaMemcpyAsync(lg + 2, c->lu.info, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
+        if ((rc = launch_axpy(p, c->force, h, dim, c->stream))) break;
+        rc = update_x_async(c, x, p, c->force, dim, h, s == steps ? -.5 : 1.0);
+    }
+    std::vector<double> lg(3 * (size_t)steps);
+    if (steps) cudaMemcpyAsync(lg.data(), c->md_log, sizeof(double) * lg.size(), cudaMemcpyDeviceToHost, c->stream);
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (rc != EPHMC_OK) return rc;
+    if (e != cudaSuccess) {
+        set_status(EPHMC_ERR_CUDA, cudaGetErrorString(e));
+        return EPHMC_ERR_CUDA;
+    }
+    unsigned neg = 0;
+    for (unsigned s = 0; s < steps; ++s) {
+        int info[2];
+        std::memcpy(info, &lg[3 * (size_t)s + 2], sizeof(info));
+        if (info[1] != 0) {
+            cudaMemsetAsync(c->lu.sync, 0, sizeof(unsigned) * lu_sync_words((int)c->V), c->stream);
+            cudaStreamSynchronize(c->stream);
+            set_status(EPHMC_ERR_TIMEOUT, "LU: a panel wait of the dataflow kernel ran out; the result is invalid");
+            return EPHMC_ERR_TIMEOUT;
+        }
+        if (info[0] != 0) {
+            set_status(EPHMC_ERR_SINGULAR, "zero pivot in an MD step");
+            return EPHMC_ERR_SINGULAR;
+        }
+        if (lg[3 * (size_t)s + 1] < 0 && (c->flavors % 2)) ++neg;
+    }
+    if (steps) {
+        c->last_logdet = lg[3 * (size_t)(steps - 1)];
+        c->last_sign = lg[3 * (size_t)(steps - 1) + 1] < 0 ? -1 : 1;
+        c->have_inverse = true;
+    }
+    if (neg) add_warning(EPHMC_WARN_NEGATIVE_DET);
+    if (negative_steps) *negative_steps = neg;
+    return EPHMC_OK;
+}
 
 // leap_frog (simulation/organic_hmc.c:167-190)
 void leap_frog(double *x, double *p, double *p_dot, ephmc_dcomplex *xc, double *M_hat, double *QM1P, double *w,

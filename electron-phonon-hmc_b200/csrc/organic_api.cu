@@ -454,14 +454,14 @@ void construct_QM1P(double *x, double *M_hat, double *QM1P, double *w, double *t
     j.p_end = kPairs;
     j.p_step = 1;
     if (after > 0) {
-        cudaMemcpy(c->jobs, &j, sizeof(j), cudaMemcpyHostToDevice);
+        ctx_upload_jobs(c, &j, 1, 0, 0);
         launch_slices<double, double, double>(Axis::Rows, X.d, c->c, c->lat, c->jobs, 1, 0);
     }
     if (time > 0) {
         j.s_first = 0;
         j.s_count = time;
         j.s_dir = 1;
-        cudaMemcpy(c->jobs, &j, sizeof(j), cudaMemcpyHostToDevice);
+        ctx_upload_jobs(c, &j, 1, 0, 0);
         launch_slices<double, double, double>(Axis::Cols, X.d, c->c, c->lat, c->jobs, 1, 0);
     }
     cudaDeviceSynchronize();

@@ -18,10 +18,11 @@
  * Pointers: every double* argument of the native surface may be a device
  * pointer (used in place) or a host pointer (staged through the context's
  * device buffers, copies included in the call).  Sizes are plain unsigned.
- * No context call allocates device memory after ephmc_ctx_create, except the
- * explicit ephmc_alloc, ephmc_ctx_set_checkpoint, and the first call of the
- * reference algorithm (its Nt V^2 G_t buffers).  The static-disorder handle grows its per-run
- * buffers on demand, and ephmc_conv_* allocate per call.
+ * No context call allocates device memory after ephmc_ctx_create, except:
+ * the explicit ephmc_alloc; ephmc_ctx_set_checkpoint; the first call of the
+ * reference algorithm (its Nt V^2 G_t buffers); and ephmc_leapfrog when it
+ * meets more steps than before (its step log).  The static-disorder handle
+ * grows its per-run buffers on demand, and ephmc_conv_* allocate per call.
  *
  * Errors: every ephmc_ function returns an ephmc_status; the most recent
  * status of the calling thread, including calls made through the drop-in
@@ -232,6 +233,21 @@ EPHMC_API int ephmc_fa_approx_step(ephmc_ctx *ctx, double *x, const double *p, d
 /* Action -flavors*logdet + energyP + (sum (dx_t)^2/omega + omega sum x^2)/2
  * (hamilton, simulation/organic_hmc.c:67-84). */
 EPHMC_API int ephmc_hamilton(ephmc_ctx *ctx, const double *x, double logdet, double energyP, double *H);
+
+/* The molecular-dynamics part of a trajectory, leap_frog
+ * (simulation/organic_hmc.c:167-190), on device x and p (3 V Nt doubles
+ * each): update_x by h/2, then per step one force+logdet evaluation,
+ * p += h p_dot and update_x by h (by -h/2 after the last), h =
+ * traj_length / steps (2 traj_length when steps = 0), with the context's
+ * Fourier-acceleration flags.  Every step is issued before any host wait;
+ * each step's log det, sign and status are read once at the end.  Afterwards
+ * the context holds the last step's inverse (ephmc_ctx_get_inverse).
+ * negative_steps (may be NULL): steps whose determinant was negative with an
+ * odd number of flavours (the reference prints "Negative determinant!" for
+ * each).  SINGLE_PARTICLE and SCHUR_FORM_INV contexts return
+ * EPHMC_ERR_UNSUPPORTED. */
+EPHMC_API int ephmc_leapfrog(ephmc_ctx *ctx, double *x, double *p, unsigned steps, double traj_length,
+                             int force_mode, unsigned *negative_steps);
 
 /* ------------------------------------------------------------------ static disorder (TL mode) */
 /* Transient-localisation histograms, the GPU form of hist_trans_loc
