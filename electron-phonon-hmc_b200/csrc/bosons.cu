@@ -191,7 +191,7 @@ int upload_modes(const std::vector<double> &h, double *scratch, cudaStream_t st,
     {
         std::lock_guard<std::mutex> l(g_tab_mu);
         auto it = g_tab.find(scratch);
-        if (it != g_tab.end() && it->second == h) return EPHMC_OK;
+        if (it != g_tab.end() && it->second == h && !uploads_are_uncached()) return EPHMC_OK;
     }
     if (int e = upload_small(scratch, h.data(), sizeof(double) * h.size(), st)) return e;
     std::lock_guard<std::mutex> l(g_tab_mu);

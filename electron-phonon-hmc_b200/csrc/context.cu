@@ -578,7 +578,7 @@ int ephmc::ctx_upload_jobs(ephmc_ctx *c, const SliceJob *jobs, int n, int slot, 
         c->jobs_host.resize(c->jobs_cap);
         c->jobs_valid.assign(c->jobs_cap, 0);
     }
-    bool same = true;
+    bool same = !uploads_are_uncached();
     for (int i = 0; i < n && same; ++i) same = c->jobs_valid[slot + i] && same_job(c->jobs_host[slot + i], jobs[i]);
     if (same) return EPHMC_OK;
     if (int e = upload_small(c->jobs + slot, jobs, sizeof(SliceJob) * n, st)) return e;
@@ -655,6 +655,7 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     for (void *b : bufs)
         if (b) cudaFree(b);
     fa_forget_tables(c->scratch);
+    if (c->lf_graph) cudaGraphExecDestroy(c->lf_graph);
     cudaFree(c->md_log);
     lu_free(c->lu);
     schur_free(c->schur);
@@ -776,6 +777,7 @@ int ephmc_ctx_create_nnt(ephmc_ctx **out, const unsigned *nnt, unsigned ns, unsi
 int ephmc_ctx_set_params(ephmc_ctx *c, const double t[3], const double kappa[3], double mu, double omega,
                          unsigned flavors) {
     if (!c || !t || !kappa) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_params");
+    ++c->param_gen;  // a captured trajectory baked the old values in
     set_couplings(c, t, kappa, mu);
     c->omega = omega;
     c->flavors = flavors;
@@ -785,6 +787,7 @@ int ephmc_ctx_set_params(ephmc_ctx *c, const double t[3], const double kappa[3],
 int ephmc_ctx_set_checkpoint(ephmc_ctx *c, unsigned interval) {
     clear_status();
     if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_checkpoint");
+    ++c->param_gen;  // a captured trajectory baked the old values in
     EPHMC_CUDA(cudaSetDevice(c->device));
     const size_t VV = (size_t)c->V * c->V;
     const size_t need = qstack_bytes_for(c->nt, interval, VV);
@@ -819,6 +822,7 @@ int ephmc_ctx_memory(const ephmc_ctx *c, size_t *bytes) {
 
 int ephmc_ctx_set_flags(ephmc_ctx *c, const ephmc_flags *flags) {
     if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_flags");
+    ++c->param_gen;  // a captured trajectory baked the old values in
     c->flags = flags ? *flags : ephmc_flags{};
     return EPHMC_OK;
 }

@@ -62,6 +62,24 @@ int build_event_tables(const unsigned *nnt, int V, std::vector<int> &ev_src,
                        std::vector<int> &ev_fac, std::vector<int> &nbr);
 void triangular_lattice(unsigned l1, unsigned l2, unsigned *nnt);
 
+// what a captured trajectory (ephmc_leapfrog_graph) depends on besides the
+// context's buffers: field pointers, steps, length, force mode and the
+// context's parameter generation
+struct LeapfrogKey {
+    double *x, *p;
+    unsigned steps;
+    double traj;
+    int mode;
+    unsigned gen;
+    bool operator==(const LeapfrogKey &o) const {
+        return x == o.x && p == o.p && steps == o.steps && traj == o.traj && mode == o.mode && gen == o.gen;
+    }
+};
+// while set on this thread, the upload caches copy every table (a stream
+// capture must record all the uploads its replays need)
+void uploads_uncached(bool on);
+bool uploads_are_uncached();
+
 // reference-algorithm buffers of a context, allocated on first use (context.cu)
 int ensure_ref_buffers(ephmc_ctx *c);
 // n slice jobs into the context's device job table at `slot`, on stream st.
@@ -277,6 +295,10 @@ struct ephmc_ctx {
     double *cc_part = nullptr;  // nt * V * 9 doubles: correlator partial sums
     double *md_log = nullptr;   // ephmc_leapfrog: per MD step log det, sign, LU status (3 doubles each)
     unsigned md_cap = 0;        // steps md_log holds
+    // ephmc_leapfrog_graph: the captured trajectory and what it was captured for
+    cudaGraphExec_t lf_graph = nullptr;
+    ephmc::LeapfrogKey lf_key{};
+    unsigned param_gen = 0;     // advanced by every change of couplings, flags or buffers
     double *scratch = nullptr;  // small device scratch (Fourier mode tables, reductions)
     size_t scratch_n = 0;
     ephmc::SchurSolver *schur = nullptr;  // SCHUR_FORM_INV eigenvalue solver, created on first use

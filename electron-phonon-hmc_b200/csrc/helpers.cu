@@ -347,6 +347,12 @@ __global__ void k_write_bytes(unsigned char *__restrict__ dst, ParamChunk c, int
 }
 }  // namespace
 
+namespace {
+thread_local bool g_uncached = false;
+}
+void uploads_uncached(bool on) { g_uncached = on; }
+bool uploads_are_uncached() { return g_uncached; }
+
 int upload_small(void *dst, const void *src, size_t bytes, cudaStream_t st) {
     const unsigned char *s = static_cast<const unsigned char *>(src);
     unsigned char *d = static_cast<unsigned char *>(dst);

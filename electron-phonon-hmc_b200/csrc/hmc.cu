@@ -274,17 +274,8 @@ short trajectory_dev(ephmc_ctx *c, double *xb, double *results, double *greens, 
     return acc;
 }
 
-}  // namespace
-
-extern "C" {
-
-// leap_frog (simulation/organic_hmc.c:167-190) on device x and p with every
-// step issued before any host wait: per step sweep 1 + LU + force, p += h F,
-// update_x.  The log det, sign and LU status of each step stay on the device
-// and are read once at the end.
-int ephmc_leapfrog(ephmc_ctx *c, double *x, double *p, unsigned steps, double traj_length, int force_mode,
-                   unsigned *negative_steps) {
-    clear_status();
+// ---------------------------------------------------------------- leapfrog pieces
+int leapfrog_prepare(ephmc_ctx *c, double *x, double *p, unsigned steps, int force_mode) {
     if (!c || !x || !p) {
         set_status(EPHMC_ERR_ARG, "ephmc_leapfrog arguments");
         return EPHMC_ERR_ARG;
@@ -313,21 +304,36 @@ int ephmc_leapfrog(ephmc_ctx *c, double *x, double *p, unsigned steps, double tr
             return EPHMC_ERR_NOMEM;
         }
         c->md_cap = steps;
+        if (c->lf_graph) {  // the step log moved
+            cudaGraphExecDestroy(c->lf_graph);
+            c->lf_graph = nullptr;
+        }
     }
+    return EPHMC_OK;
+}
+
+// every operation of the trajectory on stream st (c->stream == st), no host wait
+int leapfrog_issue(ephmc_ctx *c, double *x, double *p, unsigned steps, double traj_length, int force_mode,
+                   cudaStream_t st) {
     const size_t dim = (size_t)c->nt * c->V * 3;
     const double h = steps ? traj_length / steps : 2 * traj_length;
     int rc = update_x_async(c, x, p, c->force, dim, h, .5);
     for (unsigned s = 1; s <= steps && rc == EPHMC_OK; ++s) {
         if ((rc = eval_async(c, x, force_mode))) break;
         double *lg = c->md_log + 3 * (size_t)(s - 1);
-        cudaMemcpyAsync(lg, c->lu.diag + c->V, 2 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
-        cudaMemcpyAsync(lg + 2, c->lu.info, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->stream);
-        if ((rc = launch_axpy(p, c->force, h, dim, c->stream))) break;
+        cudaMemcpyAsync(lg, c->lu.diag + c->V, 2 * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(lg + 2, c->lu.info, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st);
+        if ((rc = launch_axpy(p, c->force, h, dim, st))) break;
         rc = update_x_async(c, x, p, c->force, dim, h, s == steps ? -.5 : 1.0);
     }
+    return rc;
+}
+
+// wait for the trajectory on st, then read each step's log det, sign and status
+int leapfrog_collect(ephmc_ctx *c, unsigned steps, int rc, cudaStream_t st, unsigned *negative_steps) {
     std::vector<double> lg(3 * (size_t)steps);
-    if (steps) cudaMemcpyAsync(lg.data(), c->md_log, sizeof(double) * lg.size(), cudaMemcpyDeviceToHost, c->stream);
-    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (steps) cudaMemcpyAsync(lg.data(), c->md_log, sizeof(double) * lg.size(), cudaMemcpyDeviceToHost, st);
+    const cudaError_t e = cudaStreamSynchronize(st);
     if (rc != EPHMC_OK) return rc;
     if (e != cudaSuccess) {
         set_status(EPHMC_ERR_CUDA, cudaGetErrorString(e));
@@ -338,8 +344,8 @@ int ephmc_leapfrog(ephmc_ctx *c, double *x, double *p, unsigned steps, double tr
         int info[2];
         std::memcpy(info, &lg[3 * (size_t)s + 2], sizeof(info));
         if (info[1] != 0) {
-            cudaMemsetAsync(c->lu.sync, 0, sizeof(unsigned) * lu_sync_words((int)c->V), c->stream);
-            cudaStreamSynchronize(c->stream);
+            cudaMemsetAsync(c->lu.sync, 0, sizeof(unsigned) * lu_sync_words((int)c->V), st);
+            cudaStreamSynchronize(st);
             set_status(EPHMC_ERR_TIMEOUT, "LU: a panel wait of the dataflow kernel ran out; the result is invalid");
             return EPHMC_ERR_TIMEOUT;
         }
@@ -357,6 +363,91 @@ int ephmc_leapfrog(ephmc_ctx *c, double *x, double *p, unsigned steps, double tr
     if (neg) add_warning(EPHMC_WARN_NEGATIVE_DET);
     if (negative_steps) *negative_steps = neg;
     return EPHMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// leap_frog (simulation/organic_hmc.c:167-190) on device x and p with every
+// step issued before any host wait: per step sweep 1 + LU + force, p += h F,
+// update_x.  The log det, sign and LU status of each step stay on the device
+// and are read once at the end.
+int ephmc_leapfrog(ephmc_ctx *c, double *x, double *p, unsigned steps, double traj_length, int force_mode,
+                   unsigned *negative_steps) {
+    clear_status();
+    int rc = leapfrog_prepare(c, x, p, steps, force_mode);
+    if (rc) return rc;
+    rc = leapfrog_issue(c, x, p, steps, traj_length, force_mode, c->stream);
+    return leapfrog_collect(c, steps, rc, c->stream, negative_steps);
+}
+
+int ephmc_leapfrog_graph(ephmc_ctx *c, double *x, double *p, unsigned steps, double traj_length, int force_mode,
+                         unsigned *negative_steps) {
+    clear_status();
+    int rc = leapfrog_prepare(c, x, p, steps, force_mode);
+    if (rc) return rc;
+    if (force_mode == EPHMC_FORCE_REFERENCE || c->flags.constant_force)
+        if ((rc = ensure_ref_buffers(c))) return rc;
+    // the graph runs on the context's private stream, ordered after the work
+    // already queued on the caller's stream and before what follows there
+    if (!c->batch_stream) {
+        if (cudaStreamCreateWithFlags(&c->batch_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->batch_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->batch_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            set_status(EPHMC_ERR_CUDA, "ephmc_leapfrog_graph: stream creation");
+            return EPHMC_ERR_CUDA;
+        }
+    }
+    cudaStream_t gs = c->batch_stream, caller = c->stream;
+    const LeapfrogKey key{x, p, steps, traj_length, force_mode, c->param_gen};
+    if (!c->lf_graph || !(c->lf_key == key)) {
+        if (c->lf_graph) cudaGraphExecDestroy(c->lf_graph);
+        c->lf_graph = nullptr;
+        cudaStream_t keep = c->stream;
+        c->stream = gs;
+        uploads_uncached(true);  // the graph must carry every table it reads
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(gs, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            rc = leapfrog_issue(c, x, p, steps, traj_length, force_mode, gs);
+            e = cudaStreamEndCapture(gs, &g);
+        }
+        uploads_uncached(false);
+        c->stream = keep;
+        if (rc == EPHMC_OK && e == cudaSuccess && g) {
+            e = cudaGraphInstantiate(&c->lf_graph, g, 0);
+            if (e != cudaSuccess) c->lf_graph = nullptr;
+        }
+        if (g) cudaGraphDestroy(g);
+        if (rc != EPHMC_OK || e != cudaSuccess || !c->lf_graph) {
+            cudaGetLastError();
+            ctx_forget_uploads(c);
+            if (rc == EPHMC_OK) {
+                char msg[200];
+                std::snprintf(msg, sizeof msg, "ephmc_leapfrog_graph: capture failed (%s)", cudaGetErrorString(e));
+                set_status(EPHMC_ERR_CUDA, msg);
+                rc = EPHMC_ERR_CUDA;
+            }
+            return rc;
+        }
+        c->lf_key = key;
+        // the captured uploads rewrote the tables: the host shadows no longer know them
+        ctx_forget_uploads(c);
+    }
+    cudaEventRecord(c->batch_ev[0], caller);
+    cudaStreamWaitEvent(gs, c->batch_ev[0], 0);
+    if (cudaGraphLaunch(c->lf_graph, gs) != cudaSuccess) {
+        cudaGetLastError();
+        set_status(EPHMC_ERR_CUDA, "ephmc_leapfrog_graph: graph launch");
+        return EPHMC_ERR_CUDA;
+    }
+    cudaEventRecord(c->batch_ev[1], gs);
+    cudaStreamWaitEvent(caller, c->batch_ev[1], 0);
+    // the tables the graph left on the device differ from what the shadows hold
+    ctx_forget_uploads(c);
+    return leapfrog_collect(c, steps, EPHMC_OK, gs, negative_steps);
 }
 
 // leap_frog (simulation/organic_hmc.c:167-190)

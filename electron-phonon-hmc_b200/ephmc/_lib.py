@@ -81,6 +81,7 @@ def load_library(path: str | None = None, build_if_missing: bool = True):
     sig("ephmc_construct_M_hat", _I, [_P, _P, _P])
     sig("ephmc_batch_eval", _I, [C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_D), _U, _I])
     sig("ephmc_leapfrog", _I, [_P, _P, _P, _U, _D, _I, C.POINTER(_U)])
+    sig("ephmc_leapfrog_graph", _I, [_P, _P, _P, _U, _D, _I, C.POINTER(_U)])
     sig("ephmc_logdet_inverse", _I, [_P, _P, _P, C.POINTER(_D), C.POINTER(_I)])
     sig("ephmc_ctx_get_inverse", _I, [_P, _P])
     sig("ephmc_ctx_last_timings", _I, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)])

@@ -139,13 +139,15 @@ class Context:
     def warnings(self):
         return self.lib.ephmc_last_warnings()
 
-    def leapfrog(self, x, p, steps, traj_length, mode="mixed"):
-        """ephmc_leapfrog on device tensors x, p (updated in place); returns
-        the number of steps with a negative determinant."""
+    def leapfrog(self, x, p, steps, traj_length, mode="mixed", graph=False):
+        """ephmc_leapfrog (or, with graph=True, ephmc_leapfrog_graph) on device
+        tensors x, p (updated in place); returns the number of steps with a
+        negative determinant."""
         m = MODES[mode] if isinstance(mode, str) else int(mode)
         neg = C.c_uint(0)
-        check(self.lib.ephmc_leapfrog(self.h, ptr(x), ptr(p), int(steps), float(traj_length), m, C.byref(neg)),
-              "ephmc_leapfrog")
+        fn = self.lib.ephmc_leapfrog_graph if graph else self.lib.ephmc_leapfrog
+        check(fn(self.h, ptr(x), ptr(p), int(steps), float(traj_length), m, C.byref(neg)),
+              "ephmc_leapfrog_graph" if graph else "ephmc_leapfrog")
         return neg.value
 
     def set_checkpoint(self, interval):

@@ -248,6 +248,14 @@ EPHMC_API int ephmc_hamilton(ephmc_ctx *ctx, const double *x, double logdet, dou
  * EPHMC_ERR_UNSUPPORTED. */
 EPHMC_API int ephmc_leapfrog(ephmc_ctx *ctx, double *x, double *p, unsigned steps, double traj_length,
                              int force_mode, unsigned *negative_steps);
+/* No counterpart in the reference.  ephmc_leapfrog as one CUDA graph: the
+ * trajectory's launches are captured at the first call for a given (x, p,
+ * steps, traj_length, force_mode) and replayed by later calls, on a stream of
+ * the context's own that is ordered after the caller's stream.  A change of
+ * couplings, flags or checkpointing makes the next call capture again.  Same
+ * results as ephmc_leapfrog; fewer host launch costs per trajectory. */
+EPHMC_API int ephmc_leapfrog_graph(ephmc_ctx *ctx, double *x, double *p, unsigned steps, double traj_length,
+                                   int force_mode, unsigned *negative_steps);
 
 /* ------------------------------------------------------------------ static disorder (TL mode) */
 /* Transient-localisation histograms, the GPU form of hist_trans_loc

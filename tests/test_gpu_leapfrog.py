@@ -81,3 +81,55 @@ def test_leapfrog_rejects_what_needs_the_host(gpu, restated):
         with pytest.raises(ephmc.EphmcError) as e:
             ctx.leapfrog(np.zeros(m.dim), np.zeros(m.dim), 2, 0.1)
         assert e.value.status == 2
+
+
+@pytest.mark.parametrize("mode", ["reference", "adjoint", "mixed"])
+def test_leapfrog_graph_equals_leapfrog(gpu, restated, mode):
+    """ephmc_leapfrog_graph against ephmc_leapfrog from the same start: the
+    first call (capture, then launch) and the second (replay) both give the
+    direct path's x and p.  After a change of the couplings the next call
+    captures again and still agrees.  Every trajectory starts from the same
+    (x, p): from this start the dynamics amplifies the rounding-level order
+    of the force's atomic sums by about 1e4 per trajectory, so chained
+    trajectories would compare nothing but that."""
+    import torch
+
+    import ephmc
+    from oracle import Model
+    m = Model.physical(12, 12, 16, 5.0)
+    x0 = restated.random_x(5, m.dim) * 0.3
+    p0 = restated.random_x(6, m.dim)
+
+    def run(ctx, graph):
+        x, p = torch.from_numpy(x0.copy()).cuda(), torch.from_numpy(p0.copy()).cuda()
+        ctx.leapfrog(x, p, 4, 0.3, mode, graph=graph)
+        return x.cpu().numpy(), p.cpu().numpy()
+
+    def close(a, b):
+        return (np.max(np.abs(a[0] - b[0])) <= 1e-12 * np.max(np.abs(b[0])) and
+                np.max(np.abs(a[1] - b[1])) <= 1e-12 * np.max(np.abs(b[1])))
+
+    with ephmc.Context(m.l1, m.l2, m.nt, m.t, m.kappa, m.mu, m.omega) as ctx:
+        ctx.fa_scale_momenta(p0)
+        # fixed buffers, as a caller replaying the graph uses them
+        xb = torch.empty(m.dim, dtype=torch.float64, device="cuda")
+        pb = torch.empty_like(xb)
+
+        def run_fixed(graph):
+            xb.copy_(torch.from_numpy(x0))
+            pb.copy_(torch.from_numpy(p0))
+            ctx.leapfrog(xb, pb, 4, 0.3, mode, graph=graph)
+            return xb.cpu().numpy(), pb.cpu().numpy()
+
+        direct = run_fixed(False)
+        first = run_fixed(True)    # capture + launch
+        second = run_fixed(True)   # replay
+        assert close(first, direct) and close(second, direct)
+        # new couplings: the captured graph is stale and must not be replayed
+        t_new = np.ascontiguousarray(0.9 * m.t)
+        k_new = np.ascontiguousarray(m.kappa)
+        ctx.lib.ephmc_ctx_set_params(ctx.h, t_new.ctypes.data, k_new.ctypes.data, m.mu, m.omega, 1)
+        direct2 = run_fixed(False)
+        assert not close(direct2, direct)
+        assert close(run_fixed(True), direct2)
+        del run
