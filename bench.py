@@ -150,6 +150,15 @@ def run_batch_bench(args):
                 if e.status != 5:
                     raise
 
+    # launch shapes per chain, by measurement (ephmc_ctx_autotune), before any timing
+    tune_gain = []
+    for c, x in zip(ctxs, xs):
+        try:
+            b, a, _ = c.autotune(x, "mixed")
+            tune_gain.append((b, a))
+        except ephmc.EphmcError as e:
+            if e.status != 5:
+                raise
     for _ in range(W):
         run_batch(xs, pds)
     run_seq()
@@ -208,6 +217,9 @@ def run_batch_bench(args):
                            "l2": "fields of all chains resident; no flush (a step touches the 64 contexts' "
                                  "buffers, several GB)"},
                 "one_chain_at_a_time": {"value": ws * K * n / seq_s, "ms_per_step": seq_s / K * 1e3},
+                "autotune": {"chains_tuned": len(tune_gain),
+                             "sum_ms_per_eval_before": sum(b for b, _ in tune_gain),
+                             "sum_ms_per_eval_after": sum(a for _, a in tune_gain)},
                 "roofline": {"bound": "fp64", "kernel": "whole batch (sweeps + LU of all chains)", "achieved": ach,
                              "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64 if fp64 else None,
                              "peak_source": "measured in this run (CUDA-core FP64 FMA probe)",

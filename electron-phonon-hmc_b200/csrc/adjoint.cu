@@ -208,7 +208,7 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     int S = 16;
     for (int o : {1, 2, 4, 8, 16})
         if ((V + o - 1) / o <= 512) { S = o; break; }
-    const int T = (((V + S - 1) / S) + 31) / 32 * 32;
+    int T = (((V + S - 1) / S) + 31) / 32 * 32;
     const size_t per_vec = 9 * (size_t)V * sizeof(Real);
     const size_t fac_b = 3 * (size_t)V * sizeof(Real);
     const size_t budget = 200 * 1024;
@@ -221,6 +221,15 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
         return EPHMC_ERR_UNSUPPORTED;
     }
     if (R > 4) R = 4;
+    // a tuned shape (ephmc_ctx_autotune) replaces the rule when it is valid
+    {
+        const int tS = lat.tune_adj_S, tR = lat.tune_adj_R;
+        if ((tS == 1 || tS == 2 || tS == 4 || tS == 8 || tS == 16) && (V + tS - 1) / tS <= 512) {
+            S = tS;
+            T = (((V + S - 1) / S) + 31) / 32 * 32;
+        }
+        if (tR >= 1 && tR <= 4 && fac_b + per_vec * tR <= budget) R = tR;
+    }
     const size_t smem = per_vec * R + fac_b;
     double pref = (double)flavors;
     if (single_particle) pref *= exp(-logdet);

@@ -809,6 +809,126 @@ int ephmc_ctx_set_checkpoint(ephmc_ctx *c, unsigned interval) {
     return EPHMC_OK;
 }
 
+// Launch shapes by measurement: each candidate is timed over a few
+// evaluations of x with the context's own phase events, and the fastest per
+// kernel stays in the context.  The candidates only change how threads and
+// CTAs share the work: every entry is summed in the same order, so log det
+// and M_hat do not change, and the force only by the order of its atomic sums.
+int ephmc_ctx_autotune(ephmc_ctx *c, const double *x, int mode, float *ms_before, float *ms_after) {
+    clear_status();
+    if (!c || !x) return ret(EPHMC_ERR_ARG, "ephmc_ctx_autotune");
+    if (mode < EPHMC_FORCE_REFERENCE || mode > EPHMC_FORCE_MIXED) return ret(EPHMC_ERR_ARG, "force mode");
+    const int V = (int)c->V;
+    // median over `reps` evaluations of the three phases
+    auto phases = [&](float out[3]) -> int {
+        const int reps = 3;
+        std::vector<float> a(reps), b(reps), d(reps);
+        double ld = 0;
+        if (int rc = ephmc_eval(c, x, nullptr, &ld, mode); rc && rc != EPHMC_ERR_NONFINITE) return rc;
+        for (int r = 0; r < reps; ++r) {
+            if (int rc = ephmc_eval(c, x, nullptr, &ld, mode); rc && rc != EPHMC_ERR_NONFINITE) return rc;
+            a[r] = c->t_mhat;
+            b[r] = c->t_lu;
+            d[r] = c->t_force;
+        }
+        for (auto *v : {&a, &b, &d}) std::sort(v->begin(), v->end());
+        out[0] = a[reps / 2];
+        out[1] = b[reps / 2];
+        out[2] = d[reps / 2];
+        return EPHMC_OK;
+    };
+    float t0[3];
+    int rc = phases(t0);
+    if (rc) return ret(rc);
+    if (ms_before) *ms_before = t0[0] + t0[1] + t0[2];
+    const bool adj = mode != EPHMC_FORCE_REFERENCE && !c->flags.constant_force;
+    const bool mixed = mode == EPHMC_FORCE_MIXED;
+    const int Ss[5] = {1, 2, 4, 8, 16}, Rs[6] = {1, 2, 3, 4, 6, 8};
+    // k_slices: M_hat unless the strip kernel builds it; the reference force's G_t passes
+    const bool slices_mhat = !(adj && slices_strip_supported(c->lat));
+    if (slices_mhat || !adj) {
+        int bS = c->lat.tune_slices_S, bR = c->lat.tune_slices_R;
+        float best = (slices_mhat ? t0[0] : 0.f) + (!adj ? t0[2] : 0.f);
+        for (int S : Ss) {
+            if ((V + S - 1) / S > 512) continue;
+            for (int R : Rs) {
+                if (((size_t)2 * R * V + 3 * (size_t)V) * sizeof(double) > 227 * 1024) continue;
+                c->lat.tune_slices_S = S;
+                c->lat.tune_slices_R = R;
+                float t[3];
+                if ((rc = phases(t))) return ret(rc);
+                const float obj = (slices_mhat ? t[0] : 0.f) + (!adj ? t[2] : 0.f);
+                if (obj < best) {
+                    best = obj;
+                    bS = S;
+                    bR = R;
+                }
+            }
+        }
+        c->lat.tune_slices_S = bS;
+        c->lat.tune_slices_R = bR;
+    }
+    // k_adjoint: the adjoint force unless the strip kernel runs it (mixed, L1 = 32)
+    if (adj && !(mixed && adjoint_strip_supported(c->lat))) {
+        float tb[3];
+        if ((rc = phases(tb))) return ret(rc);
+        int bS = c->lat.tune_adj_S, bR = c->lat.tune_adj_R;
+        float best = tb[2];
+        const size_t real = mixed ? sizeof(float) : sizeof(double);
+        for (int S : Ss) {
+            if ((V + S - 1) / S > 512) continue;
+            for (int R = 1; R <= 4; ++R) {
+                if (3 * (size_t)V * real + 9 * (size_t)V * real * R > 200 * 1024) continue;
+                c->lat.tune_adj_S = S;
+                c->lat.tune_adj_R = R;
+                float t[3];
+                if ((rc = phases(t))) return ret(rc);
+                if (t[2] < best) {
+                    best = t[2];
+                    bS = S;
+                    bR = R;
+                }
+            }
+        }
+        c->lat.tune_adj_S = bS;
+        c->lat.tune_adj_R = bR;
+    }
+    // the dataflow LU's rows per thread
+    if (V <= 1024) {
+        float tb[3];
+        if ((rc = phases(tb))) return ret(rc);
+        int best_r = c->lu.tune_rpt;
+        float best = tb[1];
+        for (int r : {1, 2, 4}) {
+            if ((V + r - 1) / r > 256) continue;
+            c->lu.tune_rpt = r;
+            float t[3];
+            if ((rc = phases(t))) return ret(rc);
+            if (t[1] < best) {
+                best = t[1];
+                best_r = r;
+            }
+        }
+        c->lu.tune_rpt = best_r;
+    }
+    ++c->param_gen;  // a captured trajectory used the old shapes
+    float t1[3];
+    if ((rc = phases(t1))) return ret(rc);
+    if (ms_after) *ms_after = t1[0] + t1[1] + t1[2];
+    return EPHMC_OK;
+}
+
+// the shapes in use: slices S, R; adjoint S, R; LU rows per thread (0 = the built-in rule)
+int ephmc_ctx_tuning(const ephmc_ctx *c, int out[5]) {
+    if (!c || !out) return ret(EPHMC_ERR_ARG, "ephmc_ctx_tuning");
+    out[0] = c->lat.tune_slices_S;
+    out[1] = c->lat.tune_slices_R;
+    out[2] = c->lat.tune_adj_S;
+    out[3] = c->lat.tune_adj_R;
+    out[4] = c->lu.tune_rpt;
+    return EPHMC_OK;
+}
+
 int ephmc_ctx_memory(const ephmc_ctx *c, size_t *bytes) {
     if (!c || !bytes) return ret(EPHMC_ERR_ARG, "ephmc_ctx_memory");
     const size_t VV = (size_t)c->V * c->V, dim = (size_t)c->nt * c->V * 3;

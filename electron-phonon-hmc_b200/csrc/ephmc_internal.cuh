@@ -55,6 +55,9 @@ struct LatticeDev {
     int *ev_fac = nullptr;
     int *nbr = nullptr;
     int *rev = nullptr;  // rev[k*V + j]: the site whose link-k neighbour is j
+    // launch shapes chosen by ephmc_ctx_autotune (0: the built-in rule):
+    // sites per thread and vectors per CTA of k_slices and of k_adjoint
+    int tune_slices_S = 0, tune_slices_R = 0, tune_adj_S = 0, tune_adj_R = 0;
 };
 
 // Host helper: build the event tables; returns EPHMC_OK or EPHMC_ERR_LATTICE.
@@ -226,6 +229,7 @@ struct LUWork {
     int *info = nullptr;       // device: [0] first zero pivot (1-based), [1] dataflow wait timed out
     double *X = nullptr;       // device V*V: panels of the dataflow kernel, or the unpermuted inverse
     unsigned *sync = nullptr;  // device, lu_sync_words(V), zeroed once: ready flags + call counter
+    int tune_rpt = 0;          // rows per thread of the dataflow kernel (ephmc_ctx_autotune; 0: built-in rule)
 };
 constexpr int kLuPanel = 8;  // columns per panel (and per CTA) of the dataflow kernel
 inline size_t lu_sync_words(int V) { return (size_t)(V + kLuPanel - 1) / kLuPanel + 1; }

@@ -686,8 +686,11 @@ int run_dataflow(double *M, LUWork &w, cudaStream_t st) {
     EPHMC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     EPHMC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) return EPHMC_ERR_UNSUPPORTED;
-    // rows per thread: at most 256 threads (8 warps) per CTA
-    const int rpt = V <= 256 ? 1 : V <= 512 ? 2 : 4;
+    // rows per thread: at most 256 threads (8 warps) per CTA; a tuned choice
+    // (ephmc_ctx_autotune) replaces the rule when it keeps to that
+    int rpt = V <= 256 ? 1 : V <= 512 ? 2 : 4;
+    if ((w.tune_rpt == 1 || w.tune_rpt == 2 || w.tune_rpt == 4) && (V + w.tune_rpt - 1) / w.tune_rpt <= 256)
+        rpt = w.tune_rpt;
     const int T = ((V + rpt - 1) / rpt + 31) / 32 * 32;
     if (rpt == 1) return launch_dataflow<1>(M, w, nblk, T, sms, st);
     if (rpt == 2) return launch_dataflow<2>(M, w, nblk, T, sms, st);

@@ -164,7 +164,10 @@ struct Shape {
     size_t smem;
 };
 
-Shape pick_shape(int V) {
+size_t shape_smem(int V, int R) { return ((size_t)2 * R * V + 3 * (size_t)V) * sizeof(double); }
+
+Shape pick_shape(const LatticeDev &lat) {
+    const int V = lat.V;
     Shape sh{};
     const int opts[5] = {1, 2, 4, 8, 16};
     sh.S = 16;
@@ -179,7 +182,14 @@ Shape pick_shape(int V) {
     if (R < 1) R = 1;
     if (R > 8) R = 8;
     sh.R = R;
-    sh.smem = ((size_t)2 * R * V + 3 * (size_t)V) * sizeof(double);
+    // a tuned shape (ephmc_ctx_autotune) replaces the rule when it is valid
+    const int tS = lat.tune_slices_S, tR = lat.tune_slices_R;
+    if ((tS == 1 || tS == 2 || tS == 4 || tS == 8 || tS == 16) && (V + tS - 1) / tS <= 512) {
+        sh.S = tS;
+        sh.T = (((V + tS - 1) / tS + 31) / 32) * 32;
+    }
+    if (tR >= 1 && shape_smem(V, tR) <= 227 * 1024) sh.R = tR;
+    sh.smem = shape_smem(V, sh.R);
     return sh;
 }
 
@@ -187,7 +197,7 @@ template <typename StackT, bool COLS>
 int launch_axis(const double *x, const Couplings &c, const LatticeDev &lat, const SliceJob *jobs,
                 int njobs, cudaStream_t st) {
     const int V = lat.V;
-    Shape sh = pick_shape(V);
+    Shape sh = pick_shape(lat);
     if (sh.smem > 227 * 1024) {
         set_status(EPHMC_ERR_UNSUPPORTED, "slice propagation: a vector and its stencil image exceed shared memory");
         return EPHMC_ERR_UNSUPPORTED;

@@ -154,6 +154,15 @@ class Context:
         """Checkpointed adjoint sweeps every `interval` slices (0: whole stack)."""
         check(self.lib.ephmc_ctx_set_checkpoint(self.h, int(interval)), "ephmc_ctx_set_checkpoint")
 
+    def autotune(self, x, mode="mixed"):
+        """ephmc_ctx_autotune on field x; returns (ms_before, ms_after, shapes)."""
+        m = MODES[mode] if isinstance(mode, str) else int(mode)
+        a, b = C.c_float(0), C.c_float(0)
+        check(self.lib.ephmc_ctx_autotune(self.h, ptr(x), m, C.byref(a), C.byref(b)), "ephmc_ctx_autotune")
+        out = (C.c_int * 5)()
+        check(self.lib.ephmc_ctx_tuning(self.h, out), "ephmc_ctx_tuning")
+        return a.value, b.value, list(out)
+
     def memory(self):
         """Device bytes the context holds."""
         b = C.c_size_t(0)

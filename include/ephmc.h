@@ -186,6 +186,19 @@ EPHMC_API int ephmc_ctx_set_flags(ephmc_ctx *ctx, const ephmc_flags *flags);
  * interval 0 restores the whole stack.  The reference algorithm's G_t
  * buffers (Nt V^2 doubles) are separate and allocated on first use. */
 EPHMC_API int ephmc_ctx_set_checkpoint(ephmc_ctx *ctx, unsigned interval);
+/* No counterpart in the reference.  Chooses the launch shapes of the
+ * thread-per-site sweeps (sites per thread, vectors per CTA) and the
+ * dataflow LU's rows per thread for this context by timing each candidate
+ * over a few evaluations of x (host or device) with force_mode, and keeps
+ * the fastest.  Sums run in the same order for every shape: log det and
+ * M_hat are unchanged.  ms_before / ms_after (may be NULL): median evaluation
+ * time before and after.  Takes a few hundred evaluations. */
+EPHMC_API int ephmc_ctx_autotune(ephmc_ctx *ctx, const double *x, int force_mode, float *ms_before,
+                                 float *ms_after);
+/* The shapes in use: out[0..1] sweep sites per thread and vectors per CTA,
+ * out[2..3] the same for the adjoint sweep, out[4] LU rows per thread
+ * (0: the built-in rule). */
+EPHMC_API int ephmc_ctx_tuning(const ephmc_ctx *ctx, int out[5]);
 /* Device bytes the context holds now (buffers allocated on first use included
  * once they exist). */
 EPHMC_API int ephmc_ctx_memory(const ephmc_ctx *ctx, size_t *bytes);
