@@ -25,6 +25,8 @@ def test_autotuned_shapes_keep_the_results(gpu, restated, shape, mode):
     print(f"{shape} {mode}: {before:.3f} -> {after:.3f} ms, shapes {shapes}")
     assert ld1 == ld0
     assert np.max(np.abs(pd1 - pd0)) <= (1e-5 if mode == "mixed" else 1e-10) * np.max(np.abs(pd0))
-    assert all(v >= 0 for v in shapes) and any(v > 0 for v in shapes)
+    # 0 keeps the rule's shape; the tuner only replaces it by a faster one
+    assert all(v >= 0 for v in shapes)
+    assert after <= 1.25 * before
     if l1 == 32:  # the strip kernels have fixed shapes: only the LU is tuned
         assert shapes[:4] == [0, 0, 0, 0]
