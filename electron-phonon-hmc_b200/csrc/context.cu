@@ -1121,7 +1121,7 @@ int ephmc_batch_eval(ephmc_ctx *const *ctxs, const double *const *x, double *con
             rc = ret(EPHMC_ERR_CUDA, "ephmc_batch_eval: stream synchronisation");
         if (rc != EPHMC_OK) continue;
         if (info[1] != 0) {
-            cudaMemsetAsync(c->lu.sync, 0, sizeof(unsigned) * lu_sync_words((int)c->V), c->stream);
+            lu_reset_sync(c->lu, c->stream);
             cudaStreamSynchronize(c->stream);
             rc = ret(EPHMC_ERR_TIMEOUT, "LU: a panel wait of the dataflow kernel ran out; the result is invalid");
             continue;

@@ -228,12 +228,18 @@ struct LUWork {
     double *diag = nullptr;    // device, U_ii
     int *info = nullptr;       // device: [0] first zero pivot (1-based), [1] dataflow wait timed out
     double *X = nullptr;       // device V*V: panels of the dataflow kernel, or the unpermuted inverse
-    unsigned *sync = nullptr;  // device, lu_sync_words(V), zeroed once: ready flags + call counter
+    // device, zeroed once: the dataflow kernel's call counter (word 0, at the
+    // same place for every V) and its ready flags; sync_words of them allocated
+    unsigned *sync = nullptr;
+    size_t sync_words = 0;
     int tune_rpt = 0;          // rows per thread of the dataflow kernel (ephmc_ctx_autotune; 0: built-in rule)
 };
 constexpr int kLuPanel = 8;  // columns per panel (and per CTA) of the dataflow kernel
-inline size_t lu_sync_words(int V) { return (size_t)(V + kLuPanel - 1) / kLuPanel + 1; }
+constexpr size_t lu_sync_words(int V) { return 1 + (size_t)(V + kLuPanel - 1) / kLuPanel; }
 int lu_alloc(LUWork &w, int V);
+// after a timed-out dataflow call: zero the counter, flags and messages (all
+// sync_words), so that no stale word matches a later call's epoch
+void lu_reset_sync(LUWork &w, cudaStream_t st);
 void lu_free(LUWork &w);
 // In-place LU with partial pivoting of the column-major matrix A(r,c) = M[c*V+r],
 // followed by the in-place inverse; log|det| and sign into host outputs.

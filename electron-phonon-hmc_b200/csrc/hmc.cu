@@ -344,7 +344,7 @@ int leapfrog_collect(ephmc_ctx *c, unsigned steps, int rc, cudaStream_t st, unsi
         int info[2];
         std::memcpy(info, &lg[3 * (size_t)s + 2], sizeof(info));
         if (info[1] != 0) {
-            cudaMemsetAsync(c->lu.sync, 0, sizeof(unsigned) * lu_sync_words((int)c->V), st);
+            lu_reset_sync(c->lu, st);
             cudaStreamSynchronize(st);
             set_status(EPHMC_ERR_TIMEOUT, "LU: a panel wait of the dataflow kernel ran out; the result is invalid");
             return EPHMC_ERR_TIMEOUT;

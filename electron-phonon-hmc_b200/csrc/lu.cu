@@ -266,11 +266,13 @@ __global__ void __launch_bounds__(256) k_gj_update(double *__restrict__ M, int V
 // also gives the dgetrf tie-break (first logical row among equal magnitudes)
 // and the final placement: the inverse is X(lpos(r), P_j) = Y(r, j), with P_j
 // the physical pivot row of step j and Y the array after the last panel.
-// The ready flags (ready[0..nblk)) carry a per-call epoch, one more than the
-// call counter ready[nblk] that every CTA reads at its start and the last
-// panel's owner advances at its end, so they are never reset and a captured
-// launch can be replayed.  Waits are bounded (kLuWaitNs): on expiry the CTA
-// sets info[1] and leaves.
+// The ready flags (sync[1..nblk]) carry a per-call epoch, one more than the
+// call counter sync[0] that every CTA reads at its start and the last panel's
+// owner advances at its end, so they are never reset and a captured launch
+// can be replayed.  The counter sits at word 0 for every V, so calls of
+// different sizes on one workspace keep counting up and no flag a smaller
+// call left behind matches a later epoch.  Waits are bounded (kLuWaitNs): on
+// expiry the CTA sets info[1] and leaves.
 constexpr unsigned long long kLuWaitNs = 2000000000ull;
 constexpr unsigned kLuWaitPolls = 1u << 26;
 
@@ -355,7 +357,7 @@ template <int NB, int RPT>
 __global__ void __launch_bounds__(256, 1) k_gj_dataflow(double *__restrict__ M, int V,
                                                         double *__restrict__ panels, int *__restrict__ ipiv,
                                                         double *__restrict__ diag, int *__restrict__ info,
-                                                        unsigned *__restrict__ ready) {
+                                                        unsigned *__restrict__ sync) {
     constexpr int MW = 8;
     // per warp candidate of a pivot step: |value| key, logical position,
     // physical row, value, and the row already divided by its pivot entry
@@ -374,6 +376,7 @@ __global__ void __launch_bounds__(256, 1) k_gj_dataflow(double *__restrict__ M, 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, T = (int)blockDim.x, NW = T >> 5;
     const int b = blockIdx.x, nblk = gridDim.x;
     const int c0 = b * NB, ncol = min(NB, V - c0);
+    unsigned *ready = sync + 1;
     int row[RPT], lpos[RPT];
     double a[RPT][NB];
 #pragma unroll
@@ -385,7 +388,7 @@ __global__ void __launch_bounds__(256, 1) k_gj_dataflow(double *__restrict__ M, 
     }
     if (tid == 0) {
         s_abort = 0;
-        const unsigned e = __ldcg(ready + nblk) + 1u;
+        const unsigned e = __ldcg(sync) + 1u;
         s_epoch = e ? e : 1u;
     }
     __syncthreads();
@@ -570,7 +573,7 @@ __global__ void __launch_bounds__(256, 1) k_gj_dataflow(double *__restrict__ M, 
             }
             diag[V] = t;
             diag[V + 1] = n ? -1.0 : 1.0;
-            ready[nblk] = epoch;
+            sync[0] = epoch;
         }
     }
 }
@@ -679,7 +682,7 @@ int launch_dataflow(double *M, LUWork &w, int nblk, int T, int sms, cudaStream_t
 // EPHMC_ERR_UNSUPPORTED (nothing launched) when they are not, or V > 1024.
 int run_dataflow(double *M, LUWork &w, cudaStream_t st) {
     const int V = w.V;
-    if (V > 1024 || w.sync == nullptr) return EPHMC_ERR_UNSUPPORTED;
+    if (V > 1024 || w.sync == nullptr || w.sync_words < lu_sync_words(V)) return EPHMC_ERR_UNSUPPORTED;
     const int nblk = (V + kLuPanel - 1) / kLuPanel;
     int dev = 0, sms = 0, coop = 0;
     EPHMC_CUDA(cudaGetDevice(&dev));
@@ -705,9 +708,14 @@ int lu_alloc(LUWork &w, int V) {
     EPHMC_CUDA(cudaMalloc(&w.diag, sizeof(double) * (V + 2)));
     EPHMC_CUDA(cudaMalloc(&w.info, sizeof(int) * 2));
     EPHMC_CUDA(cudaMalloc(&w.X, sizeof(double) * (size_t)V * V));
-    EPHMC_CUDA(cudaMalloc(&w.sync, sizeof(unsigned) * lu_sync_words(V)));
-    EPHMC_CUDA(cudaMemset(w.sync, 0, sizeof(unsigned) * lu_sync_words(V)));
+    w.sync_words = lu_sync_words(V);
+    EPHMC_CUDA(cudaMalloc(&w.sync, sizeof(unsigned) * w.sync_words));
+    EPHMC_CUDA(cudaMemset(w.sync, 0, sizeof(unsigned) * w.sync_words));
     return EPHMC_OK;
+}
+
+void lu_reset_sync(LUWork &w, cudaStream_t st) {
+    if (w.sync && w.sync_words) cudaMemsetAsync(w.sync, 0, sizeof(unsigned) * w.sync_words, st);
 }
 
 void lu_free(LUWork &w) {
@@ -762,7 +770,7 @@ int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv
     if (sign) *sign = ld[1] < 0 ? -1 : 1;
     if (info[1] != 0) {
         // flags of the abandoned call could match the next call's epoch
-        cudaMemsetAsync(w.sync, 0, sizeof(unsigned) * lu_sync_words(V), st);
+        lu_reset_sync(w, st);
         cudaStreamSynchronize(st);
         set_status(EPHMC_ERR_TIMEOUT, "LU: a panel wait of the dataflow kernel ran out; the result is invalid");
         return EPHMC_ERR_TIMEOUT;

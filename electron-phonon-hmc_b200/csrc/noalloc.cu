@@ -33,7 +33,7 @@ constexpr size_t kOffDiag = kOffX + align256(sizeof(double) * kNoAllocMaxN * kNo
 constexpr size_t kOffIpiv = kOffDiag + align256(sizeof(double) * (kNoAllocMaxN + 2));
 constexpr size_t kOffInfo = kOffIpiv + align256(sizeof(int) * 2 * kNoAllocMaxN);  // pivots + permutation
 constexpr size_t kOffSync = kOffInfo + align256(sizeof(int) * 2);
-constexpr size_t kNoAllocBytes = kOffSync + align256(sizeof(unsigned) * ((kNoAllocMaxN + ephmc::kLuPanel - 1) / ephmc::kLuPanel + 1));
+constexpr size_t kNoAllocBytes = kOffSync + align256(sizeof(unsigned) * ephmc::lu_sync_words(kNoAllocMaxN));
 
 // Host code must not take this symbol's address directly (that is a host-side
 // stand-in); the device address comes from cudaGetSymbolAddress below.
@@ -94,6 +94,7 @@ EPHMC_API int ephmc_logdet_inverse_noalloc(double *M, unsigned n, double *logdet
     w.ipiv = reinterpret_cast<int *>(base + kOffIpiv);
     w.info = reinterpret_cast<int *>(base + kOffInfo);  // zeroed by the factorisation itself
     w.sync = reinterpret_cast<unsigned *>(base + kOffSync);  // zero-initialised with the module
+    w.sync_words = ephmc::lu_sync_words(kNoAllocMaxN);
     int sg = 1;
     double ld = 0;
     rc = ephmc::lu_logdet_inverse(M, w, &ld, &sg, ipiv, static_cast<cudaStream_t>(stream));

@@ -60,3 +60,24 @@ def test_noalloc_rejects_oversize(gpu):
     st, _, _, _ = _noalloc(lib, Md, 257)
     assert st == 2
     assert b"256" in lib.ephmc_last_error_message()
+
+
+def test_noalloc_alternating_sizes(gpu):
+    """Calls of different sizes share the static workspace: 256, 128, 256, 64,
+    256 in a row, each against numpy.  The LU kernel's call counter sits at the
+    same word for every size, so the panel flags and messages that a smaller
+    call leaves behind never carry the epoch of a later, larger call."""
+    import torch
+    lib = _lib()
+    rng = np.random.default_rng(7)
+    for n in (256, 128, 256, 64, 256, 128):
+        A = rng.standard_normal((n, n)) + 3.0 * np.eye(n)
+        Md = torch.from_numpy(A.copy()).cuda()
+        st, ld, sg, ipiv = _noalloc(lib, Md, n)
+        assert st == 0, lib.ephmc_last_error_message()
+        s_np, ld_np = np.linalg.slogdet(A.T)  # the LU sees the transpose (column-major)
+        assert abs(ld - ld_np) <= 1e-11 * abs(ld_np), n
+        assert sg == int(s_np), n
+        inv = Md.cpu().numpy()
+        ref = np.linalg.inv(A)
+        assert np.max(np.abs(inv - ref)) <= 1e-10 * np.max(np.abs(ref)), n
