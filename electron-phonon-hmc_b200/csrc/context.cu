@@ -900,7 +900,7 @@ int ephmc_ctx_autotune(ephmc_ctx *c, const double *x, int mode, float *ms_before
         int best_r = c->lu.tune_rpt;
         float best = tb[1];
         for (int r : {1, 2, 4}) {
-            if ((V + r - 1) / r > 256) continue;
+            if (!lu_shape_ok((int)V, r)) continue;
             c->lu.tune_rpt = r;
             float t[3];
             if ((rc = phases(t))) return ret(rc);

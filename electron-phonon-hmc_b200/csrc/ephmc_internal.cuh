@@ -237,6 +237,8 @@ struct LUWork {
 constexpr int kLuPanel = 8;  // columns per panel (and per CTA) of the dataflow kernel
 constexpr size_t lu_sync_words(int V) { return 1 + (size_t)(V + kLuPanel - 1) / kLuPanel; }
 int lu_alloc(LUWork &w, int V);
+// rpt rows per thread is one of the dataflow kernel's shapes for V
+bool lu_shape_ok(int V, int rpt);
 // after a timed-out dataflow call: zero the counter, flags and messages (all
 // sync_words), so that no stale word matches a later call's epoch
 void lu_reset_sync(LUWork &w, cudaStream_t st);

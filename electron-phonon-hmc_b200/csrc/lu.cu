@@ -352,13 +352,13 @@ __device__ __forceinline__ void rotate_left(double (&a)[NB]) {
     a[NB - 1] = t;
 }
 
-// RPT rows per thread (rows tid, tid + T, ...), T = blockDim.x <= 256.
-template <int NB, int RPT>
-__global__ void __launch_bounds__(256, 1) k_gj_dataflow(double *__restrict__ M, int V,
+// RPT rows per thread (rows tid, tid + T, ...), T = blockDim.x <= MAXT.
+template <int NB, int RPT, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) k_gj_dataflow(double *__restrict__ M, int V,
                                                         double *__restrict__ panels, int *__restrict__ ipiv,
                                                         double *__restrict__ diag, int *__restrict__ info,
                                                         unsigned *__restrict__ sync) {
-    constexpr int MW = 8;
+    constexpr int MW = MAXT / 32;
     // per warp candidate of a pivot step: |value| key, logical position,
     // physical row, value, and the row already divided by its pivot entry
     __shared__ unsigned long long ck[2][MW];
@@ -664,19 +664,35 @@ int run_panels(double *M, LUWork &w, cudaStream_t st) {
     return EPHMC_OK;
 }
 
-template <int RPT>
+template <int RPT, int MAXT>
 int launch_dataflow(double *M, LUWork &w, int nblk, int T, int sms, cudaStream_t st) {
     int per_sm = 0;
-    EPHMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_dataflow<kLuPanel, RPT>, T, 0));
+    EPHMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_dataflow<kLuPanel, RPT, MAXT>, T, 0));
     if ((long)per_sm * sms < nblk) return EPHMC_ERR_UNSUPPORTED;
     const int V = w.V;
     double *panels = w.X;
     void *args[] = {&M, (void *)&V, &panels, &w.ipiv, &w.diag, &w.info, &w.sync};
-    EPHMC_CUDA(cudaLaunchCooperativeKernel((const void *)k_gj_dataflow<kLuPanel, RPT>, dim3(nblk), dim3(T), args, 0,
-                                           st));
+    EPHMC_CUDA(cudaLaunchCooperativeKernel((const void *)k_gj_dataflow<kLuPanel, RPT, MAXT>, dim3(nblk), dim3(T), args,
+                                           0, st));
     ephmc::count_launch(1);
     return EPHMC_OK;
 }
+
+// CTA sizes of the dataflow kernel for a given number of rows per thread:
+// 256 threads at most, or 512 with 2 rows per thread.  At V = 1024, 512
+// threads of 2 rows (128 registers each) take 1.31 ms against 1.45 for 256
+// threads of 4 rows: each pivot step's row scan and rank-1 update are half as
+// long per thread, with twice the warps to hide them; 1024 threads of one row
+// (64 registers) take 1.82 ms.
+inline int lu_max_threads(int rpt) { return rpt == 2 ? 512 : 256; }
+
+}  // namespace
+
+bool lu_shape_ok(int V, int rpt) {
+    return (rpt == 1 || rpt == 2 || rpt == 4) && (V + rpt - 1) / rpt <= lu_max_threads(rpt);
+}
+
+namespace {
 
 // The dataflow kernel needs all ceil(V/8) CTAs resident at once; returns
 // EPHMC_ERR_UNSUPPORTED (nothing launched) when they are not, or V > 1024.
@@ -689,15 +705,15 @@ int run_dataflow(double *M, LUWork &w, cudaStream_t st) {
     EPHMC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     EPHMC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) return EPHMC_ERR_UNSUPPORTED;
-    // rows per thread: at most 256 threads (8 warps) per CTA; a tuned choice
-    // (ephmc_ctx_autotune) replaces the rule when it keeps to that
-    int rpt = V <= 256 ? 1 : V <= 512 ? 2 : 4;
-    if ((w.tune_rpt == 1 || w.tune_rpt == 2 || w.tune_rpt == 4) && (V + w.tune_rpt - 1) / w.tune_rpt <= 256)
-        rpt = w.tune_rpt;
+    // rows per thread; a tuned choice (ephmc_ctx_autotune) replaces the rule
+    // when its CTA size is one of the kernel's
+    int rpt = V <= 256 ? 1 : 2;
+    if (lu_shape_ok(V, w.tune_rpt)) rpt = w.tune_rpt;
     const int T = ((V + rpt - 1) / rpt + 31) / 32 * 32;
-    if (rpt == 1) return launch_dataflow<1>(M, w, nblk, T, sms, st);
-    if (rpt == 2) return launch_dataflow<2>(M, w, nblk, T, sms, st);
-    return launch_dataflow<4>(M, w, nblk, T, sms, st);
+    if (rpt == 1) return launch_dataflow<1, 256>(M, w, nblk, T, sms, st);
+    if (rpt == 2) return T > 256 ? launch_dataflow<2, 512>(M, w, nblk, T, sms, st)
+                                 : launch_dataflow<2, 256>(M, w, nblk, T, sms, st);
+    return launch_dataflow<4, 256>(M, w, nblk, T, sms, st);
 }
 
 }  // namespace
