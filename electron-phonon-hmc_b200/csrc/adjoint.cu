@@ -35,8 +35,11 @@ __device__ __forceinline__ Real stencil_at(const Real *__restrict__ v, int j, co
 
 // SEG: a segment of a checkpointed sweep (AdjointRange); without it the
 // kernel walks all slices from M^-1 and the range fields are not read
-template <typename Real, typename QT, int S, bool SEG>
-__global__ void __launch_bounds__(512) k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
+// WIDE: at most 320 threads, so that S = 8 sites keep their tables in 168
+// registers instead of spilling (the FP32 force at 48x48, Nt = 128: 27.2 ms
+// instead of 39.5)
+template <typename Real, typename QT, int S, bool SEG, bool WIDE = false>
+__global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
                           const int *__restrict__ ev_fac, const int *__restrict__ nbr,
                           const QT *__restrict__ qstack, const double *__restrict__ Minv, int V, int nt,
                           int R, double pref_scale, double *__restrict__ force, AdjointRange rg_in) {
@@ -243,7 +246,10 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
         case 1: kern = seg ? k_adjoint<Real, QT, 1, true> : k_adjoint<Real, QT, 1, false>; break;
         case 2: kern = seg ? k_adjoint<Real, QT, 2, true> : k_adjoint<Real, QT, 2, false>; break;
         case 4: kern = seg ? k_adjoint<Real, QT, 4, true> : k_adjoint<Real, QT, 4, false>; break;
-        case 8: kern = seg ? k_adjoint<Real, QT, 8, true> : k_adjoint<Real, QT, 8, false>; break;
+        case 8:
+            if (T <= 320) kern = seg ? k_adjoint<Real, QT, 8, true, true> : k_adjoint<Real, QT, 8, false, true>;
+            else kern = seg ? k_adjoint<Real, QT, 8, true> : k_adjoint<Real, QT, 8, false>;
+            break;
         default: kern = seg ? k_adjoint<Real, QT, 16, true> : k_adjoint<Real, QT, 16, false>; break;
     }
     EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
