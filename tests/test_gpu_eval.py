@@ -102,7 +102,7 @@ def test_cfg0_literal_reproduces_reference_behaviour(gpu, restated):
 def test_lu_against_numpy(gpu):
     import ephmc
     rng = np.random.default_rng(0)
-    for V, (l1, l2) in ((36, (6, 6)), (256, (16, 16)), (1024, (32, 32))):
+    for V, (l1, l2) in ((36, (6, 6)), (256, (16, 16)), (1024, (32, 32)), (1600, (40, 40)), (2304, (48, 48))):
         A = rng.standard_normal((V, V)) + 3 * np.eye(V)
         with ephmc.Context(l1, l2, 1, [0.1, 0.1, 0.1], [0, 0, 0], -1.0, 0.1) as ctx:
             M = A.copy()
