@@ -25,7 +25,8 @@ REFERENCE_SO = os.path.join(HERE, "_ref", "libephref.so")
 
 _D, _U, _P, _I = C.c_double, C.c_uint, C.c_void_p, C.c_int
 
-# BASELINE parameters in physical units (organic_main input.txt semantics)
+# couplings of the benchmark workloads in physical units (organic_main input.txt
+# semantics): J, lambda, mu0, omega0
 J_DEFAULT = (1.0, -0.5, -0.5)
 LAMBDA_DEFAULT = (0.3, 0.15, 0.15)
 MU0_DEFAULT = -3.0
