@@ -62,9 +62,10 @@ def test_eval_fp64_matches_reference(gpu, restated, name, mode):
 @pytest.mark.parametrize("name", WELL)
 def test_eval_mixed_error_is_bounded(gpu, restated, name):
     """FP64 M_hat/LU/logdet, FP32 force sweep: log det exact to FP64, force
-    error stated against the FP64 force.  The FP32 error grows on small
-    lattices at small Nt, where the force is a sum of few large terms that
-    cancel (1e-6 at 6x6, Nt=16 up to 1.2e-4 at 2x2, Nt=4)."""
+    error stated against the FP64 force.  The force is a sum over vectors
+    whose single terms exceed |G_t| by 1e4-1e6 (the propagator chains are not
+    stabilised, in the reference neither), so FP32 inputs to that cancelling
+    sum bound the error from below: 1e-6 at 6x6, Nt=16, 1.2e-4 at 2x2, Nt=4."""
     g = golden(f"eval_{name}.npz")
     m = model_from_golden(g)
     with ctx_for(g) as ctx:
