@@ -175,7 +175,7 @@ size_t fa_smem(int n, bool two) {
     return sizeof(double) * (2 * (size_t)n + (two ? 2 : 1) * (size_t)n * kTile + (two ? 4 : 2) * (size_t)nc * kTile);
 }
 
-// freq2_k = omega + (2 sin(pi k / Nt))^2 / omega   (simulation/organic_bosons.c:134)
+// freq2_k = omega + (2 sin(pi k / Nt))^2 / omega   (simulation/organic_bosons.c:136)
 double freq2(double omega, int k, int n) {
     const double matsubara = 3.141592653589793 / n;  // M_PI, simulation/organic_aux.h:7
     return omega + std::pow(2 * std::sin(matsubara * k), 2) / omega;

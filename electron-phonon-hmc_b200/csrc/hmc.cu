@@ -256,7 +256,7 @@ short trajectory_dev(ephmc_ctx *c, double *xb, double *results, double *greens, 
             results[5] = (!mode.zero_filling && !mode.single_particle) ? 1 - tr / ns : tr / ns;
             results[6] = acc;
             results[7] = boltzmann;
-            // average_links (simulation/organic_aux.c:129-140): sum over slices and sites / ns
+            // average_links (simulation/organic_aux.c:199-210): sum over slices and sites / ns
             std::vector<double> xh(dim);
             cudaMemcpy(xh.data(), x, sizeof(double) * dim, cudaMemcpyDeviceToHost);
             for (unsigned k = 0; k < 3; ++k) results[8 + k] = 0;

@@ -8,7 +8,7 @@ import numpy as np
 
 from ._lib import MODES, Flags, check, load_library, ptr
 
-ROOM_TEMPERATURE = 0.025  # simulation/organic_main.c:8
+ROOM_TEMPERATURE = 0.025  # simulation/organic_main.c:17
 
 
 def convert_params(beta, nt, J, lam, mu0, omega0, static_disorder=False):

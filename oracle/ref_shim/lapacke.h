@@ -7,7 +7,7 @@
  * are declared:
  *   dgetrf / dgetri  simulation/organic_dense_matrix.c:580,595
  *   dgees            simulation/organic_dense_matrix.c:560
- *   dsyev            simulation/organic_trans_loc.c:223
+ *   dsyev            simulation/organic_trans_loc.c:40
  * This file is test infrastructure, not part of the shipped library.
  */
 #ifndef EPHMC_ORACLE_LAPACKE_SHIM_H
