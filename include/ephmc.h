@@ -190,8 +190,10 @@ EPHMC_API int ephmc_ctx_set_checkpoint(ephmc_ctx *ctx, unsigned interval);
  * thread-per-site sweeps (sites per thread, vectors per CTA) and the
  * dataflow LU's rows per thread for this context by timing each candidate
  * over a few evaluations of x (host or device) with force_mode, and keeps
- * the fastest.  Sums run in the same order for every shape: log det and
- * M_hat are unchanged.  ms_before / ms_after (may be NULL): median evaluation
+ * the fastest.  The sweeps sum in the same order for every shape (M_hat is
+ * unchanged); the LU's pivots and inverse are unchanged, and its log det is
+ * summed over terms grouped by the CTA size, so a new LU shape can move it
+ * in the last bit.  ms_before / ms_after (may be NULL): median evaluation
  * time before and after.  Takes a few hundred evaluations. */
 EPHMC_API int ephmc_ctx_autotune(ephmc_ctx *ctx, const double *x, int force_mode, float *ms_before,
                                  float *ms_after);
