@@ -120,11 +120,14 @@ def test_lu_against_numpy(gpu):
             assert np.array_equal(ipiv - 1, piv)
 
 
-@pytest.mark.parametrize("kind", ["permutation", "ones_plus_identity", "small_integers"])
+@pytest.mark.parametrize("kind", ["permutation", "ones_plus_identity", "small_integers", "ones_minus_identity"])
 def test_lu_ties_follow_lapack(gpu, kind):
-    """Matrices with many equal magnitudes in a pivot column: the pivot rows
-    are dgetrf's (first logical row among equal magnitudes), so ipiv equals
-    scipy's LAPACK getrf and the inverse is exact to rounding."""
+    """Structured matrices: the pivot rows are dgetrf's, so ipiv equals
+    scipy's LAPACK getrf and the inverse is exact to rounding.  Only
+    ones_minus_identity reaches a tie (column 0 holds 0 above V-1 equal ones):
+    there the pivot is the first logical row among equal magnitudes; rows
+    with equal values get identical updates, so the tie is exact in any
+    arithmetic.  The others have a unique largest entry at every step."""
     import ephmc
     import scipy.linalg as sl
     rng = np.random.default_rng(11)
@@ -133,6 +136,8 @@ def test_lu_ties_follow_lapack(gpu, kind):
         A = np.eye(V)[rng.permutation(V)]
     elif kind == "ones_plus_identity":
         A = np.ones((V, V)) + np.eye(V)
+    elif kind == "ones_minus_identity":
+        A = np.ones((V, V)) - np.eye(V)
     else:
         A = rng.integers(-2, 3, size=(V, V)).astype(float) + 6 * np.eye(V)
     with ephmc.Context(4, 4, 1, [0.1, 0.1, 0.1], [0, 0, 0], -1.0, 0.1) as ctx:
