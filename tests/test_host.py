@@ -42,3 +42,18 @@ def test_host_convert_params_equals_the_oracle(beta, nt, static):
     b = oracle.convert_params(beta, nt, J, lam, mu0, om0, static_disorder=static)
     for x, y in zip(a, b):
         assert np.array_equal(np.asarray(x), np.asarray(y))
+
+
+def test_no_gpu_fails_loudly():
+    """Without a CUDA device every handle's creation raises EphmcError with the
+    library's status and message: nothing falls back to a CPU path."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    import ephmc
+    t, kappa, mu, omega = ephmc.convert_params(10.0, 16, (1.0, -0.5, -0.5), (0.3, 0.15, 0.15), -3.0, 0.05)
+    with pytest.raises(ephmc.EphmcError, match="ephmc_ctx_create"):
+        ephmc.Context(4, 4, 16, t, kappa, mu, omega)
+    cm = ephmc.contraction_matrix((1.0, 0.0), (0.5, 0.8660254))
+    with pytest.raises(ephmc.EphmcError, match="ephmc_tl_create"):
+        ephmc.TransLoc(4, 4, 16, t, kappa, mu, cm)
