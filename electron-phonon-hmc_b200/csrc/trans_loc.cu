@@ -404,6 +404,11 @@ int tl_create_nnt(ephmc_tl **out, const unsigned *nnt, unsigned V, unsigned nbin
     std::vector<int> rv(3 * (size_t)V, 0);
     for (unsigned k = 0; k < 3; ++k)
         for (unsigned i = 0; i < V; ++i) rv[(size_t)k * V + nb[(size_t)k * V + i]] = (int)i;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return tl_fail(EPHMC_ERR_NO_DEVICE, "no CUDA device");
+    }
     if (device < 0) EPHMC_CUDA(cudaGetDevice(&device));
     EPHMC_CUDA(cudaSetDevice(device));
     ephmc_tl *tl = new (std::nothrow) ephmc_tl();
