@@ -154,6 +154,12 @@ struct ConvBufs {
 
 int conv_upload(ConvBufs &b, const double *sigma, unsigned n, const double *widths, unsigned ns, size_t nout,
                 size_t nterms) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_status(EPHMC_ERR_NO_DEVICE, "no CUDA device");
+        return EPHMC_ERR_NO_DEVICE;
+    }
     if (cudaMalloc(&b.sigma, sizeof(double) * n) != cudaSuccess ||
         cudaMalloc(&b.widths, sizeof(double) * ns) != cudaSuccess ||
         cudaMalloc(&b.out, sizeof(double) * nout) != cudaSuccess ||

@@ -57,3 +57,8 @@ def test_no_gpu_fails_loudly():
     cm = ephmc.contraction_matrix((1.0, 0.0), (0.5, 0.8660254))
     with pytest.raises(ephmc.EphmcError, match="ephmc_tl_create: status 9"):
         ephmc.TransLoc(4, 4, 16, t, kappa, mu, cm)
+    sigma, widths = np.ones(16), np.array([0.1])
+    with pytest.raises(ephmc.EphmcError, match="status 9"):
+        ephmc.conv_sigma_w(sigma, 0.1, widths)
+    with pytest.raises(ephmc.EphmcError, match="status 9"):
+        ephmc.conv_sigma_t(sigma, 0.1, widths, 8)
