@@ -124,10 +124,11 @@ def test_lu_against_numpy(gpu):
 def test_lu_ties_follow_lapack(gpu, kind):
     """Structured matrices: the pivot rows are dgetrf's, so ipiv equals
     scipy's LAPACK getrf and the inverse is exact to rounding.  Only
-    ones_minus_identity reaches a tie (column 0 holds 0 above V-1 equal ones):
-    there the pivot is the first logical row among equal magnitudes; rows
-    with equal values get identical updates, so the tie is exact in any
-    arithmetic.  The others have a unique largest entry at every step."""
+    ones_minus_identity reaches ties: at steps 0 and 1 all 15 candidates are
+    exactly 1, and the pivot is the first logical row among them; at every
+    later step the largest entry leads the next by at least half its size
+    (exact rational elimination), so rounding cannot change the sequence.
+    The others have a unique largest entry at every step."""
     import ephmc
     import scipy.linalg as sl
     rng = np.random.default_rng(11)
