@@ -33,18 +33,32 @@ __device__ __forceinline__ Real stencil_at(const Real *__restrict__ v, int j, co
     return acc;
 }
 
-// SEG: a segment of a checkpointed sweep (AdjointRange); without it the
-// kernel walks all slices from M^-1 and the range fields are not read
+// MODE 0: all slices from M^-1 (the range fields are not read); 1: one
+// segment of a checkpointed sweep (AdjointRange t0, t1, q_top, y_in, y_out);
+// 2: the segment grid (AdjointRange seg_*), one segment per blockIdx.y
 // WIDE: at most 320 threads, so that S = 8 sites keep their tables in 168
 // registers instead of spilling (the FP32 force at 48x48, Nt = 128: 27.2 ms
 // instead of 39.5)
-template <typename Real, typename QT, int S, bool SEG, bool WIDE = false>
+template <typename Real, typename QT, int S, int MODE, bool WIDE = false>
 __global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
                           const int *__restrict__ ev_fac, const int *__restrict__ nbr,
                           const QT *__restrict__ qstack, const double *__restrict__ Minv, int V, int nt,
                           int R, double pref_scale, double *__restrict__ force, AdjointRange rg_in) {
     AdjointRange rg = rg_in;
-    if (!SEG) rg = AdjointRange{0, nt, nullptr, nullptr, nullptr, true};
+    if (MODE == 0) rg = AdjointRange{0, nt, nullptr, nullptr, nullptr, true};
+    // the segment of the grid (MODE 2): slices [t0, t1), identity q at t1 - 1
+    int q_id_slice = nt - 1;
+    if (MODE == 2) {
+        const int j = rg.seg_j0 + (int)blockIdx.y;
+        rg.t1 = nt - j * rg.seg_C;
+        rg.t0 = max(0, rg.t1 - rg.seg_C);
+        q_id_slice = rg.t1 - 1;
+        qstack += rg.seg_regions ? (size_t)j * rg.seg_C * V * V : 0;
+        rg.y_start += rg.seg_regions ? (size_t)j * V * V : 0;
+        rg.q_top = nullptr;
+        rg.y_out = nullptr;
+        rg.y_in = nullptr;
+    }
     extern __shared__ unsigned char smem_raw[];
     Real *base = reinterpret_cast<Real *>(smem_raw);
     const size_t RV = (size_t)R * V;
@@ -70,9 +84,12 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *_
         for (int k = 0; k < 3; ++k) nb[s][k] = (j < V) ? nbr[k * V + j] : 0;
     }
 
-    // y(t0): row c of M^-1 (math) = column c of the inverse's array, or the
-    // rows a previous segment left in rg.y_in
-    if (rg.y_in != nullptr) {
+    // y(t0): row c of M^-1 (math) = column c of the inverse's array, the rows
+    // a previous segment left in rg.y_in, or the segment's FP64 start rows
+    if (MODE == 2) {
+        const double *yi = rg.y_start + (size_t)c0 * V;
+        for (int f = tid; f < nvec * V; f += T) y[f] = (Real)yi[f];
+    } else if (rg.y_in != nullptr) {
         const Real *yi = static_cast<const Real *>(rg.y_in) + (size_t)c0 * V;
         for (int f = tid; f < nvec * V; f += T) y[f] = yi[f];
     } else {
@@ -89,7 +106,7 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *_
             const int k = e % 3;
             fac[e] = (Real)fma(-c.kappa[k], xs[e], c.t[k]);
         }
-        if (t == nt - 1) {
+        if (t == q_id_slice) {
             for (int f = tid; f < nvec * V; f += T) {
                 const int r = f / V, j = f % V;
                 q[f] = (j == c0 + r) ? (Real)1 : (Real)0;
@@ -195,7 +212,7 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *_
         y = yn;
         yn = tmp;
     }
-    if (rg.y_out != nullptr) {
+    if (MODE != 2 && rg.y_out != nullptr) {
         Real *yo = static_cast<Real *>(rg.y_out) + (size_t)c0 * V;
         for (int f = tid; f < nvec * V; f += T) yo[f] = y[f];
     }
@@ -206,7 +223,7 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *_
 template <typename Real, typename QT>
 int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat, const QT *qstack,
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
-                         double *force, cudaStream_t st, const AdjointRange *range) {
+                         double *force, cudaStream_t st, const AdjointRange *range, int seg_count) {
     const int V = lat.V;
     int S = 16;
     for (int o : {1, 2, 4, 8, 16})
@@ -241,20 +258,24 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     if (rg.zero_force) EPHMC_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * (size_t)nt * V * 3, st));
     void (*kern)(const double *, Couplings, const int *, const int *, const int *, const QT *, const double *,
                  int, int, int, double, double *, AdjointRange) = nullptr;
-    const bool seg = range != nullptr;
+    const int mode = rg.seg_C > 0 ? 2 : range != nullptr ? 1 : 0;
+#define EPHMC_ADJ_PICK(SS, ...)                                                              \
+    (mode == 2 ? k_adjoint<Real, QT, SS, 2, ##__VA_ARGS__>                                  \
+               : mode == 1 ? k_adjoint<Real, QT, SS, 1, ##__VA_ARGS__> : k_adjoint<Real, QT, SS, 0, ##__VA_ARGS__>)
     switch (S) {
-        case 1: kern = seg ? k_adjoint<Real, QT, 1, true> : k_adjoint<Real, QT, 1, false>; break;
-        case 2: kern = seg ? k_adjoint<Real, QT, 2, true> : k_adjoint<Real, QT, 2, false>; break;
-        case 4: kern = seg ? k_adjoint<Real, QT, 4, true> : k_adjoint<Real, QT, 4, false>; break;
+        case 1: kern = EPHMC_ADJ_PICK(1); break;
+        case 2: kern = EPHMC_ADJ_PICK(2); break;
+        case 4: kern = EPHMC_ADJ_PICK(4); break;
         case 8:
-            if (T <= 320) kern = seg ? k_adjoint<Real, QT, 8, true, true> : k_adjoint<Real, QT, 8, false, true>;
-            else kern = seg ? k_adjoint<Real, QT, 8, true> : k_adjoint<Real, QT, 8, false>;
+            if (T <= 320) kern = EPHMC_ADJ_PICK(8, true);
+            else kern = EPHMC_ADJ_PICK(8);
             break;
-        default: kern = seg ? k_adjoint<Real, QT, 16, true> : k_adjoint<Real, QT, 16, false>; break;
+        default: kern = EPHMC_ADJ_PICK(16); break;
     }
+#undef EPHMC_ADJ_PICK
     EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<(V + R - 1) / R, T, smem, st>>>(x, c, lat.ev_src, lat.ev_fac, lat.nbr, qstack, Minv, V, nt, R, pref,
-                                           force, rg);
+    const dim3 grid((V + R - 1) / R, mode == 2 ? (unsigned)seg_count : 1u);
+    kern<<<grid, T, smem, st>>>(x, c, lat.ev_src, lat.ev_fac, lat.nbr, qstack, Minv, V, nt, R, pref, force, rg);
     ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
     return EPHMC_OK;
@@ -262,9 +283,9 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
 
 template int launch_adjoint_sweep<double, double>(const double *, const Couplings &, const LatticeDev &,
                                                   const double *, const double *, int, unsigned, int, double,
-                                                  double *, cudaStream_t, const AdjointRange *);
+                                                  double *, cudaStream_t, const AdjointRange *, int);
 template int launch_adjoint_sweep<float, float>(const double *, const Couplings &, const LatticeDev &,
                                                 const float *, const double *, int, unsigned, int, double,
-                                                double *, cudaStream_t, const AdjointRange *);
+                                                double *, cudaStream_t, const AdjointRange *, int);
 
 }  // namespace ephmc

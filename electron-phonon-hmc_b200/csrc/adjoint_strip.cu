@@ -119,16 +119,17 @@ __device__ __forceinline__ P link_term(const Site &i, const Site &n, P aq0, P aq
 
 __device__ __forceinline__ double pick3(const double (&a)[3], int k) { return k == 0 ? a[0] : k == 1 ? a[1] : a[2]; }
 
-// SEG: a segment of a checkpointed sweep (AdjointRange); without it the
-// kernel walks all slices from M^-1 and the range fields are not read
-template <bool SEG>
+// MODE 0: all slices from M^-1 (the range fields are not read); 1: one
+// segment of a checkpointed sweep (AdjointRange t0, t1, q_top, y_in, y_out);
+// 2: the segment grid (AdjointRange seg_*), one segment per blockIdx.y
+template <int MODE>
 __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restrict__ x, Couplings cp,
                                                           const float *__restrict__ qstack,
                                                           const double *__restrict__ Minv, int L2, int nt,
                                                           double pref, double *__restrict__ force,
                                                           AdjointRange rg_in) {
     AdjointRange rg = rg_in;
-    if (!SEG) rg = AdjointRange{0, nt, nullptr, nullptr, nullptr, true};
+    if (MODE == 0) rg = AdjointRange{0, nt, nullptr, nullptr, nullptr, true};
     extern __shared__ float sm[];
     const int V = 32 * L2, nw = L2 / kH;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -147,16 +148,31 @@ __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restri
     const size_t VV = (size_t)V * V;
     // V = 32 L2 is a multiple of the 4 vectors of a CTA: every vector is live
     const int cv0 = (blockIdx.x * kG + g) * kR, cv1 = cv0 + 1;
+    // the segment of the grid (MODE 2): slices [t0, t1), identity q at t1 - 1
+    int q_id_slice = nt - 1;
+    if (MODE == 2) {
+        const int j = rg.seg_j0 + (int)blockIdx.y;
+        rg.t1 = nt - j * rg.seg_C;
+        rg.t0 = max(0, rg.t1 - rg.seg_C);
+        q_id_slice = rg.t1 - 1;
+        qstack += rg.seg_regions ? (size_t)j * rg.seg_C * VV : 0;
+        rg.y_start += rg.seg_regions ? (size_t)j * VV : 0;
+        rg.q_top = nullptr;
+        rg.y_out = nullptr;
+    }
 
-    // y(t0): rows cv0, cv1 of M^-1 (columns of the inverse's array), or the
-    // rows a previous segment left in rg.y_in
+    // y(t0): rows cv0, cv1 of M^-1 (columns of the inverse's array), the rows
+    // a previous segment left in rg.y_in, or the segment's FP64 start rows
     const float *y_in = static_cast<const float *>(rg.y_in);
     P y[kH];
 #pragma unroll
     for (int h = 0; h < kH; ++h) {
         const int i = (b0 + h) * 32 + lane;
-        y[h] = y_in ? make_float2(y_in[(size_t)cv0 * V + i], y_in[(size_t)cv1 * V + i])
-                    : make_float2((float)Minv[(size_t)i * V + cv0], (float)Minv[(size_t)i * V + cv1]);
+        if (MODE == 2)
+            y[h] = make_float2((float)rg.y_start[(size_t)cv0 * V + i], (float)rg.y_start[(size_t)cv1 * V + i]);
+        else
+            y[h] = y_in ? make_float2(y_in[(size_t)cv0 * V + i], y_in[(size_t)cv1 * V + i])
+                        : make_float2((float)Minv[(size_t)i * V + cv0], (float)Minv[(size_t)i * V + cv1]);
     }
     for (int e = threadIdx.x; e < 6 * V; e += blockDim.x) acc[e] = 0.f;
     __syncthreads();
@@ -187,7 +203,8 @@ __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restri
             }
         }
         // q(t): the stack entry t - t0, the segment's FP64 checkpoint (its last
-        // slice, checkpointed evaluation), or e_c (slice nt-1)
+        // slice, checkpointed evaluation), or e_c (slice nt-1; the top slice of
+        // a segment of the grid)
         P q[kH];
         {
             const bool top = rg.q_top != nullptr && t == rg.t1 - 1;
@@ -195,7 +212,7 @@ __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restri
 #pragma unroll
             for (int h = 0; h < kH; ++h) {
                 const int i = (b0 + h) * 32 + lane;
-                q[h] = (t == nt - 1) ? make_float2(i == cv0 ? 1.f : 0.f, i == cv1 ? 1.f : 0.f)
+                q[h] = (t == q_id_slice) ? make_float2(i == cv0 ? 1.f : 0.f, i == cv1 ? 1.f : 0.f)
                        : top ? make_float2((float)rg.q_top[(size_t)cv0 * V + i], (float)rg.q_top[(size_t)cv1 * V + i])
                              : make_float2(__ldg(qs + (size_t)cv0 * V + i), __ldg(qs + (size_t)cv1 * V + i));
             }
@@ -287,7 +304,7 @@ __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restri
             acc_t[e] = 0.f;
         }
     }
-    if (rg.y_out != nullptr) {
+    if (MODE != 2 && rg.y_out != nullptr) {
         float *y_out = static_cast<float *>(rg.y_out);
 #pragma unroll
         for (int h = 0; h < kH; ++h) {
@@ -306,7 +323,7 @@ bool adjoint_strip_supported(const LatticeDev &lat) {
 
 int launch_adjoint_strip(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
-                         double *force, cudaStream_t st, const AdjointRange *range) {
+                         double *force, cudaStream_t st, const AdjointRange *range, int seg_count) {
     if (!adjoint_strip_supported(lat)) return EPHMC_ERR_UNSUPPORTED;
     const int V = lat.V, L2 = lat.l2, nw = L2 / kH;
     const size_t smem = sizeof(float) * (6 * (size_t)V + 2 * (size_t)kG * kSlots * kR * nw * 32);
@@ -317,15 +334,11 @@ int launch_adjoint_strip(const double *x, const Couplings &c, const LatticeDev &
     if (range) rg = *range;
     if (rg.zero_force) EPHMC_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * (size_t)nt * V * 3, st));
     const int per_cta = kG * kR;
-    if (range) {
-        EPHMC_CUDA(cudaFuncSetAttribute(k_adjoint_strip<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_adjoint_strip<true><<<(V + per_cta - 1) / per_cta, kG * nw * 32, smem, st>>>(x, c, qstack, Minv, L2, nt,
-                                                                                     pref, force, rg);
-    } else {
-        EPHMC_CUDA(cudaFuncSetAttribute(k_adjoint_strip<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_adjoint_strip<false><<<(V + per_cta - 1) / per_cta, kG * nw * 32, smem, st>>>(x, c, qstack, Minv, L2, nt,
-                                                                                      pref, force, rg);
-    }
+    const dim3 grid((V + per_cta - 1) / per_cta, rg.seg_C > 0 ? (unsigned)seg_count : 1u);
+    void (*kern)(const double *, Couplings, const float *, const double *, int, int, double, double *,
+                 AdjointRange) = rg.seg_C > 0 ? k_adjoint_strip<2> : range ? k_adjoint_strip<1> : k_adjoint_strip<0>;
+    EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, kG * nw * 32, smem, st>>>(x, c, qstack, Minv, L2, nt, pref, force, rg);
     ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
     return EPHMC_OK;

@@ -2,6 +2,8 @@
 // buffers and the three force+logdet algorithms.
 #include "ephmc_internal.cuh"
 
+#include <cublas_v2.h>
+
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -247,12 +249,12 @@ double *ckpt_state(ephmc_ctx *c, int j) {
 
 void *ckpt_segment(ephmc_ctx *c, size_t m) { return static_cast<double *>(c->qstack) + (m - 1) * c->V * c->V; }
 
-int launch_sweep1(ephmc_ctx *c, const double *x, const SliceJob *jobs_dev, bool stack_float) {
+int launch_sweep1(ephmc_ctx *c, const double *x, const SliceJob *jobs_dev, bool stack_float, int n = 1) {
     if (slices_strip_supported(c->lat))
-        return stack_float ? launch_slices_strip<float>(x, c->c, c->lat, jobs_dev, 1, c->stream)
-                           : launch_slices_strip<double>(x, c->c, c->lat, jobs_dev, 1, c->stream);
-    if (stack_float) return launch_slices<double, double, float>(Axis::Rows, x, c->c, c->lat, jobs_dev, 1, c->stream);
-    return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, jobs_dev, 1, c->stream);
+        return stack_float ? launch_slices_strip<float>(x, c->c, c->lat, jobs_dev, n, c->stream)
+                           : launch_slices_strip<double>(x, c->c, c->lat, jobs_dev, n, c->stream);
+    if (stack_float) return launch_slices<double, double, float>(Axis::Rows, x, c->c, c->lat, jobs_dev, n, c->stream);
+    return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, jobs_dev, n, c->stream);
 }
 
 // sweep 1 keeping only the checkpoints: one launch per segment, the FP64 state
@@ -314,8 +316,232 @@ int adjoint_ckpt(ephmc_ctx *c, const double *x, const double *y0, bool mixed, do
     return rc;
 }
 
+// ------------------------------------------------------------------ segmented mixed force
+// The mixed force splits the slice chain into segments of C slices (the
+// checkpoint interval when one is set, else ephmc_ctx_set_segment's length,
+// else min(16, max(1, Nt/4))): segment j covers [b_{j+1}, b_j),
+// b_j = max(0, Nt - jC).
+// For t in a segment [t0, t1) the reference's G_t = Q_t M^-1 P_t is
+//   G_t = L_t Z R_t,  L_t = B_{t+1}...B_{t1-1},  R_t = B_{t0}...B_{t-1},
+//   Z = Q_{t1-1} M^-1 P_{t0},
+// so with q'_c(t) = L_t e_c and y'_c(t) = R_t^T Z^T e_c the sweep-2 kernels
+// contract the same formulas over each segment independently.  Z is formed in
+// FP64: Q_{t1-1} is sweep 1's FP64 state at b_j, the rows of M^-1 P_{t0} come
+// from an FP64 y chain, and y'(t0) = Q_{t1-1}^T (M^-1 P_{t0}) is one GEMM per
+// segment.  Only L_t and R_t run in FP32, so the terms of the FP32 sum over
+// vectors grow over C slices of the chain instead of Nt, and the cancellation
+// that bounded the unsegmented FP32 force (4e-3 at 32x32, Nt = 64) stays at
+// the size of one segment's growth (6e-7 in an FP64/FP32 numpy model).
+constexpr size_t kBlasWorkspace = (size_t)32 << 20;  // cuBLAS workspace of the Z GEMMs
+
+struct SegPlan {
+    int C = 0, m = 0;
+    std::vector<int> b;   // b[0] = nt > b[1] > ... > b[m] = 0
+    bool regions = true;  // one FP32 stack region per segment (else one, reused)
+};
+
+unsigned seg_length(const ephmc_ctx *c) {
+    if (c->ckpt) return std::min(c->ckpt, c->nt);
+    if (c->seg_len) return std::min(c->seg_len, c->nt);
+    return std::min(16u, std::max(1u, c->nt / 4));
+}
+
+SegPlan seg_plan(const ephmc_ctx *c) {
+    SegPlan p;
+    p.C = (int)seg_length(c);
+    p.b = ckpt_bounds(c->nt, (unsigned)p.C);
+    p.m = (int)p.b.size() - 1;
+    p.regions = c->ckpt == 0;
+    return p;
+}
+
+// Buffers.  Regions: c->seg = [ck_1..ck_{m-1}][ys_1..ys_{m-1}][ys_0 = yst_0][yst_1..yst_{m-1}],
+// the FP32 stack regions in c->qstack.  Checkpointed: ck_j are the context's
+// checkpoints, one FP32 region after them, and the y chain and one segment's
+// start rows live in c->work (no segment buffer).  ck_j: FP64 rows of
+// Q_{b_j} = B_{b_j}...B_{Nt-1} (j = 1..m-1); ys_j: FP64 rows of
+// M^-1 P_{b_{j+1}} (ys_{m-1}: M^-1 itself, transposed); yst_j: y'(b_{j+1}) of
+// segment j.
+size_t seg_doubles(const SegPlan &p, size_t VV) { return p.regions ? VV * (3 * (size_t)p.m - 2) : 0; }
+
+double *seg_ck(ephmc_ctx *c, const SegPlan &p, int j) {
+    const size_t VV = (size_t)c->V * c->V;
+    return p.regions ? c->seg + (size_t)(j - 1) * VV : ckpt_state(c, j);
+}
+double *seg_ys(ephmc_ctx *c, const SegPlan &p, int j) {
+    const size_t VV = (size_t)c->V * c->V;
+    return c->seg + (size_t)(j == 0 ? 2 * p.m - 2 : p.m + j - 2) * VV;
+}
+double *seg_yst(ephmc_ctx *c, const SegPlan &p, int j) {
+    const size_t VV = (size_t)c->V * c->V;
+    return j == 0 ? seg_ys(c, p, 0) : c->seg + (size_t)(2 * p.m - 2 + j) * VV;
+}
+float *seg_region(ephmc_ctx *c, const SegPlan &p, int j) {
+    const size_t VV = (size_t)c->V * c->V;
+    if (p.regions) return static_cast<float *>(c->qstack) + (size_t)j * p.C * VV;
+    return static_cast<float *>(ckpt_segment(c, (size_t)p.m));
+}
+
+int ensure_seg(ephmc_ctx *c, const SegPlan &p) {
+    const size_t need = sizeof(double) * seg_doubles(p, (size_t)c->V * c->V);
+    if (3 * p.m > c->jobs_cap) return ret(EPHMC_ERR_ARG, "segment length too small for Nt");
+    if (c->seg_bytes != need) {
+        cudaFree(c->seg);
+        c->seg = nullptr;
+        c->seg_bytes = 0;
+        if (need && cudaMalloc((void **)&c->seg, need) != cudaSuccess) {
+            cudaGetLastError();
+            c->seg = nullptr;
+            return ret(EPHMC_ERR_NOMEM, "segmented force buffers");
+        }
+        c->seg_bytes = need;
+    }
+    if (!c->blas) {
+        cublasHandle_t h = nullptr;
+        if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) return ret(EPHMC_ERR_CUDA, "cublasCreate");
+        c->blas = h;
+        // an explicit workspace, so that no GEMM of a captured trajectory allocates
+        if (cudaMalloc(&c->blas_ws, kBlasWorkspace) != cudaSuccess) {
+            cudaGetLastError();
+            c->blas_ws = nullptr;
+            return ret(EPHMC_ERR_NOMEM, "cuBLAS workspace");
+        }
+    }
+    cublasHandle_t h = static_cast<cublasHandle_t>(c->blas);
+    if (cublasSetStream(h, c->stream) != CUBLAS_STATUS_SUCCESS ||
+        cublasSetWorkspace(h, c->blas_ws, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS)
+        return ret(EPHMC_ERR_CUDA, "cublasSetStream / cublasSetWorkspace");
+    return EPHMC_OK;
+}
+
+// rows of the jobs on the context's lattice: the register-strip kernel where it applies
+int launch_rows(ephmc_ctx *c, const double *x, const SliceJob *jobs_dev, int n) {
+    if (slices_strip_supported(c->lat)) return launch_slices_strip<double>(x, c->c, c->lat, jobs_dev, n, c->stream);
+    return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, jobs_dev, n, c->stream);
+}
+
+// FP32 stacks from the identity at the top of segment j (j >= 1; segment 0's
+// stack is spilled by sweep 1): q'(t) = B_{t+1}...B_{t1-1} into its region
+SliceJob seg_identity_job(ephmc_ctx *c, const SegPlan &p, int j) {
+    const int t0 = p.b[j + 1], t1 = p.b[j];
+    SliceJob jb = job(nullptr, nullptr, t1 - 1, t1 - t0 - 1, -1, 0, kPairs, 1);
+    jb.stack = seg_region(c, p, j);
+    jb.stack_off = -1 - t0;
+    return jb;
+}
+
+// Sweep 1 of the segmented force: M_hat into dst in FP64, the FP64 states at
+// the segment boundaries (one launch per segment, the state passed through
+// memory, the same arithmetic as the whole chain), segment 0's FP32 stack
+// spilled on the way, and (regions) the other segments' FP32 stacks from the
+// identity in one more launch.
+int sweep1_seg(ephmc_ctx *c, const double *x, double *dst) {
+    const SegPlan p = seg_plan(c);
+    int rc;
+    if ((rc = ensure_seg(c, p))) return rc;
+    std::vector<SliceJob> v;
+    for (int j = 0; j < p.m; ++j) {
+        SliceJob jb = job(j == 0 ? nullptr : seg_ck(c, p, j), j == p.m - 1 ? dst : seg_ck(c, p, j + 1), p.b[j] - 1,
+                          p.b[j] - p.b[j + 1], -1, 0, kPairs, 1);
+        jb.add_identity = (j == p.m - 1) && !(c->flags.zero_filling || c->flags.single_particle);
+        if (j == 0 && p.regions) {
+            jb.stack = seg_region(c, p, 0);
+            jb.stack_off = -1 - p.b[1];
+        }
+        v.push_back(jb);
+    }
+    if ((rc = upload_jobs(c, v, c->jobs))) return rc;
+    for (int j = 0; j < p.m && rc == EPHMC_OK; ++j) rc = launch_sweep1(c, x, c->jobs + j, j == 0);
+    if (rc || !p.regions) return rc;
+    std::vector<SliceJob> id;
+    for (int j = 1; j < p.m; ++j)
+        if (p.b[j] - p.b[j + 1] > 1) id.push_back(seg_identity_job(c, p, j));
+    if (id.empty()) return EPHMC_OK;
+    if ((rc = upload_jobs(c, id, c->jobs + p.m))) return rc;
+    return launch_sweep1(c, x, c->jobs + p.m, true, (int)id.size());
+}
+
+// y'(t0) of n segments: yst = ck^T ys (row-major V x V), the n operands and
+// results each V^2 apart.  In cuBLAS's column-major view a row-major X is
+// X^T, so yst^T = ys^T ck  <=>  C = A B^T with A = ys, B = ck as stored.
+int seg_gemm(ephmc_ctx *c, const double *ys, const double *ck, double *yst, int n) {
+    const int V = (int)c->V;
+    const long long VV = (long long)V * V;
+    const double one = 1.0, zero = 0.0;
+    cublasHandle_t h = static_cast<cublasHandle_t>(c->blas);
+    cublasStatus_t st;
+    if (n == 1)
+        st = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, V, V, V, &one, ys, V, ck, V, &zero, yst, V);
+    else
+        st = cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_T, V, V, V, &one, ys, V, VV, ck, V, VV, &zero, yst,
+                                       V, VV, n);
+    count_launch((unsigned)n);
+    if (st != CUBLAS_STATUS_SUCCESS) return ret(EPHMC_ERR_CUDA, "cublasDgemm (segment start rows)");
+    return EPHMC_OK;
+}
+
+// Sweep 2 of the segmented force (after sweep1_seg and the LU): y0 is the
+// FP64 matrix whose rows start the y chain (M^-1 as the inverse's array,
+// or the identity for SINGLE_PARTICLE).
+int force_mixed_seg(ephmc_ctx *c, const double *x, const double *y0, double logdet) {
+    const SegPlan p = seg_plan(c);
+    const int V = (int)c->V;
+    const size_t VV = (size_t)V * V;
+    const ephmc_flags &f = c->flags;
+    int rc;
+    if ((rc = ensure_seg(c, p))) return rc;
+    AdjointRange rg{0, 0, nullptr, nullptr, nullptr, true};
+    rg.seg_C = p.C;
+    rg.seg_regions = p.regions;
+    auto adjoint = [&](int count) {
+        if (adjoint_strip_supported(c->lat))
+            return launch_adjoint_strip(x, c->c, c->lat, seg_region(c, p, 0), y0, (int)c->nt, c->flavors,
+                                        f.single_particle, logdet, c->force, c->stream, &rg, count);
+        return launch_adjoint_sweep<float, float>(x, c->c, c->lat, seg_region(c, p, 0), y0, (int)c->nt, c->flavors,
+                                                  f.single_particle, logdet, c->force, c->stream, &rg, count);
+    };
+    if (p.regions) {
+        // FP64 y chain: ys_{m-1} = rows of M^-1, then forward through each
+        // segment; all segments' start rows by one batched GEMM; one launch
+        // for all segments
+        if ((rc = launch_transpose_rect(y0, seg_ys(c, p, p.m - 1), V, V, c->stream))) return rc;
+        std::vector<SliceJob> v;
+        for (int j = p.m - 2; j >= 0; --j)
+            v.push_back(job(seg_ys(c, p, j + 1), seg_ys(c, p, j), p.b[j + 2], p.b[j + 1] - p.b[j + 2], +1, 1, -1, -1));
+        if ((rc = upload_jobs(c, v, c->jobs + 2 * p.m))) return rc;
+        for (int k = 0; k < p.m - 1 && rc == EPHMC_OK; ++k) rc = launch_rows(c, x, c->jobs + 2 * p.m + k, 1);
+        if (rc) return rc;
+        if (p.m > 1 && (rc = seg_gemm(c, seg_ys(c, p, 1), seg_ck(c, p, 1), seg_yst(c, p, 1), p.m - 1))) return rc;
+        rg.seg_j0 = 0;
+        rg.y_start = seg_yst(c, p, 0);
+        return adjoint(p.m);
+    }
+    // checkpointed: one FP32 region, reused, segments bottom up; the y chain
+    // advances in place in work[2V^2, 3V^2), a segment's start rows go to
+    // work[3V^2, 4V^2), and every segment's stack is recomputed from the
+    // identity just before its sweep
+    double *Y = c->work + 2 * VV, *yst = c->work + 3 * VV;
+    if ((rc = launch_transpose_rect(y0, Y, V, V, c->stream))) return rc;
+    std::vector<SliceJob> v;
+    for (int j = 0; j < p.m; ++j) v.push_back(seg_identity_job(c, p, j));
+    for (int j = p.m - 2; j >= 0; --j) v.push_back(job(Y, Y, p.b[j + 2], p.b[j + 1] - p.b[j + 2], +1, 1, -1, -1));
+    if ((rc = upload_jobs(c, v, c->jobs + p.m))) return rc;
+    const SliceJob *id_jobs = c->jobs + p.m, *y_jobs = c->jobs + 2 * p.m;
+    for (int j = p.m - 1; j >= 0 && rc == EPHMC_OK; --j) {
+        if (j < p.m - 1 && (rc = launch_rows(c, x, y_jobs + (p.m - 2 - j), 1))) break;
+        if (j > 0 && (rc = seg_gemm(c, Y, seg_ck(c, p, j), yst, 1))) break;
+        if (p.b[j] - p.b[j + 1] > 1 && (rc = launch_sweep1(c, x, id_jobs + j, true))) break;
+        rg.seg_j0 = j;
+        rg.zero_force = j == p.m - 1;
+        rg.y_start = j > 0 ? yst : Y;
+        rc = adjoint(1);
+    }
+    return rc;
+}
+
 // M_hat (or, with a stack, sweep 1 of the adjoint) into dst (default c->M)
 int build_M_hat(ephmc_ctx *c, const double *x, void *stack, bool stack_float, double *dst = nullptr) {
+    if (stack && stack_float) return sweep1_seg(c, x, dst ? dst : c->M);
     if (stack && c->ckpt) return build_M_hat_ckpt(c, x, stack_float, dst ? dst : c->M);
     SliceJob j = job(nullptr, dst ? dst : c->M, (int)c->nt - 1, (int)c->nt, -1, 0, kPairs, 1);
     j.add_identity = !(c->flags.zero_filling || c->flags.single_particle);
@@ -522,7 +748,9 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
             if ((rc = launch_identity(c->work, (int)c->V, c->stream))) return rc;
             y0 = c->work;
         }
-        if (c->ckpt)
+        if (mixed)
+            rc = force_mixed_seg(c, xd, y0, logdet);
+        else if (c->ckpt)
             rc = adjoint_ckpt(c, xd, y0, mixed, logdet);
         else if (!mixed)
             rc = launch_adjoint_sweep<double, double>(xd, c->c, c->lat, static_cast<const double *>(c->qstack), y0,
@@ -550,6 +778,7 @@ int force_core(ephmc_ctx *c, const double *xd, const double *Minv, double logdet
 }  // namespace
 
 int ephmc::ensure_ref_buffers(ephmc_ctx *c) { return ensure_ref(c); }
+int ephmc::ensure_seg_buffers(ephmc_ctx *c) { return ensure_seg(c, seg_plan(c)); }
 
 // One evaluation issued on the context stream without a host wait: sweep 1,
 // LU (log det, sign and status stay in c->lu), force into c->force.  For the
@@ -659,6 +888,9 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     cudaFree(c->md_log);
     lu_free(c->lu);
     schur_free(c->schur);
+    if (c->seg) cudaFree(c->seg);
+    if (c->blas) cublasDestroy(static_cast<cublasHandle_t>(c->blas));
+    if (c->blas_ws) cudaFree(c->blas_ws);
     if (c->batch_stream) cudaStreamDestroy(c->batch_stream);
     for (cudaEvent_t e : c->batch_ev)
         if (e) cudaEventDestroy(e);
@@ -707,7 +939,7 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     c->lat.l2 = (int)l2;
     const size_t VV = (size_t)V * V, dim = (size_t)nt * V * 3;
     c->refine_batch = (int)std::min<unsigned>(nt, 16);
-    c->jobs_cap = (int)std::max<unsigned>(2 * nt, 2 * (unsigned)c->refine_batch) + 8;
+    c->jobs_cap = (int)std::max<unsigned>(3 * nt, 2 * (unsigned)c->refine_batch) + 8;
     c->scratch_n = fa_scratch_doubles(3 * (int)V, (int)nt) + 16 + kActionScratch;
     auto fail = [&](cudaError_t e, const char *what) {
         cuda_fail(e, what);
@@ -806,6 +1038,16 @@ int ephmc_ctx_set_checkpoint(ephmc_ctx *c, unsigned interval) {
         c->qstack_bytes = need;
     }
     c->ckpt = interval;
+    return EPHMC_OK;
+}
+
+int ephmc_ctx_set_segment(ephmc_ctx *c, unsigned length) {
+    clear_status();
+    if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_segment");
+    const unsigned C = length ? std::min(length, c->nt) : 0;
+    if (C && 3 * ((c->nt + C - 1) / C) > (unsigned)c->jobs_cap) return ret(EPHMC_ERR_ARG, "segment length too small for Nt");
+    ++c->param_gen;  // a captured trajectory baked the old segments in
+    c->seg_len = C;
     return EPHMC_OK;
 }
 
@@ -936,6 +1178,7 @@ int ephmc_ctx_memory(const ephmc_ctx *c, size_t *bytes) {
     if (c->G) b += sizeof(double) * VV * c->nt;
     if (c->A) b += 2 * sizeof(double) * VV * c->refine_batch;
     b += sizeof(double) * VV + sizeof(int) * ((size_t)c->V + lu_sync_words((int)c->V));  // LU panel store, pivots
+    b += c->seg_bytes + (c->blas_ws ? kBlasWorkspace : 0);  // segmented mixed force
     *bytes = b;
     return EPHMC_OK;
 }

@@ -85,6 +85,8 @@ bool uploads_are_uncached();
 
 // reference-algorithm buffers of a context, allocated on first use (context.cu)
 int ensure_ref_buffers(ephmc_ctx *c);
+// buffers and cuBLAS handle of the segmented mixed force, allocated on first use (context.cu)
+int ensure_seg_buffers(ephmc_ctx *c);
 // n slice jobs into the context's device job table at `slot`, on stream st.
 // Entries the table already holds are not copied again: a copy from pageable
 // host memory first waits for the stream to drain, so repeated evaluations
@@ -123,11 +125,22 @@ struct AdjointRange {
     const void *y_in;
     void *y_out;
     bool zero_force;  // clear the force first (the first segment only)
+    // Segment grid (seg_C > 0; t0, t1, q_top, y_in, y_out unused): segment
+    // j = seg_j0 + blockIdx.y covers slices [max(0, nt - (j+1) C), nt - j C).
+    // Its q at the top slice is e_c, its other q(t) are entry t - t0 of stack
+    // region (seg_regions ? j : 0) (C entries of V^2 each), and its y starts
+    // from the FP64 rows y_start + (seg_regions ? j : 0) V^2.  Segments are
+    // independent: the segment's G_t = L_t Z_j R_t with Z_j = Q_top M^-1 P_t0
+    // carried in its y start.
+    int seg_C = 0, seg_j0 = 0;
+    bool seg_regions = false;
+    const double *y_start = nullptr;
 };
 
 struct SliceJob {
     const void *src;       // input matrix; nullptr = start from the identity
-    void *dst;             // output matrix (may equal src)
+    void *dst;             // output matrix (may equal src); nullptr: the state after
+                           // the last slice goes to the stack like the others
     void *stack;           // optional: state after slice s goes to stack[(s + stack_off) * V*V]
     int stack_off;
     int s_first, s_count, s_dir;  // slices s_first, s_first + s_dir, ...
@@ -166,14 +179,15 @@ template <typename Real, typename QT>
 int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat,
                          const QT *qstack, const double *Minv, int nt, unsigned flavors,
                          int single_particle, double logdet, double *force, cudaStream_t st,
-                         const AdjointRange *range = nullptr);
+                         const AdjointRange *range = nullptr, int seg_count = 1);
 
 // FP32 adjoint sweep 2 for L1 = 32 lattices with the lattice in registers
 // (adjoint_strip.cu)
 bool adjoint_strip_supported(const LatticeDev &lat);
 int launch_adjoint_strip(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
-                         double *force, cudaStream_t st, const AdjointRange *range = nullptr);
+                         double *force, cudaStream_t st, const AdjointRange *range = nullptr,
+                         int seg_count = 1);
 
 // ---------------------------------------------------------------- drop-in helpers (helpers.cu)
 // out = (mu + K) in on nvec rows (or columns) of V x V matrices, reference order;
@@ -314,6 +328,14 @@ struct ephmc_ctx {
     double *scratch = nullptr;  // small device scratch (Fourier mode tables, reductions)
     size_t scratch_n = 0;
     ephmc::SchurSolver *schur = nullptr;  // SCHUR_FORM_INV eigenvalue solver, created on first use
+    // segmented mixed force (context.cu): FP64 segment-boundary states, the y
+    // chain at the segment starts and the segments' y starts, allocated on
+    // first use; the cuBLAS handle of its Z GEMMs and that handle's workspace
+    unsigned seg_len = 0;       // ephmc_ctx_set_segment (0: the built-in rule)
+    double *seg = nullptr;
+    size_t seg_bytes = 0;
+    void *blas = nullptr;       // cublasHandle_t
+    void *blas_ws = nullptr;
     // ephmc_batch_eval: the context's own non-blocking stream, used in place of
     // the legacy default stream so that chains overlap; created on first use
     cudaStream_t batch_stream = nullptr;

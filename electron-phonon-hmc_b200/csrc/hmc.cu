@@ -389,6 +389,8 @@ int ephmc_leapfrog_graph(ephmc_ctx *c, double *x, double *p, unsigned steps, dou
     if (rc) return rc;
     if (force_mode == EPHMC_FORCE_REFERENCE || c->flags.constant_force)
         if ((rc = ensure_ref_buffers(c))) return rc;
+    if (force_mode == EPHMC_FORCE_MIXED && !c->flags.constant_force)
+        if ((rc = ensure_seg_buffers(c))) return rc;
     // the graph runs on the context's private stream, ordered after the work
     // already queued on the caller's stream and before what follows there
     if (!c->batch_stream) {

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, WIDE ? 1 : 2) k_slices(const
             }
             __syncthreads();
         }
-        if (job.stack != nullptr && it + 1 < job.s_count) {
+        if (job.stack != nullptr && (it + 1 < job.s_count || job.dst == nullptr)) {
             StackT *dst = static_cast<StackT *>(job.stack) + (size_t)(sl + job.stack_off) * VV;
             if (!COLS) {
                 for (int f = tid; f < nvec * V; f += T) st_as<StackT>(dst, (size_t)vec0 * V + f, v[f]);
@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, WIDE ? 1 : 2) k_slices(const
         }
     }
     __syncthreads();
+    if (job.dst == nullptr) return;
     if (job.add_identity) {
         for (int r = tid; r < nvec; r += T) v[(size_t)r * V + vec0 + r] += 1.0;
         __syncthreads();

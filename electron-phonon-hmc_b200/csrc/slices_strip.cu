@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(256) k_slices_strip(const double *__restrict__
                     for (int h = 0; h < H; ++h) v[r][h] = fma(al, w[r][h], v[r][h]);
             }
         }
-        if (job.stack != nullptr && it + 1 < job.s_count) {
+        if (job.stack != nullptr && (it + 1 < job.s_count || job.dst == nullptr)) {
             StackT *dst = static_cast<StackT *>(job.stack) + (size_t)(sl + job.stack_off) * VV;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -158,6 +158,7 @@ __global__ void __launch_bounds__(256) k_slices_strip(const double *__restrict__
         }
     }
     double *dst = static_cast<double *>(job.dst);
+    if (dst == nullptr) return;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int c = vec0 + r;

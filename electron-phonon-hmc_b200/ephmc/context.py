@@ -150,6 +150,10 @@ class Context:
               "ephmc_leapfrog_graph" if graph else "ephmc_leapfrog")
         return neg.value
 
+    def set_segment(self, length):
+        """Segment length of the mixed force (0: the built-in min(Nt, 16))."""
+        check(self.lib.ephmc_ctx_set_segment(self.h, int(length)), "ephmc_ctx_set_segment")
+
     def set_checkpoint(self, interval):
         """Checkpointed adjoint sweeps every `interval` slices (0: whole stack)."""
         check(self.lib.ephmc_ctx_set_checkpoint(self.h, int(interval)), "ephmc_ctx_set_checkpoint")

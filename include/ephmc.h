@@ -20,8 +20,10 @@
  * device buffers, copies included in the call).  Sizes are plain unsigned.
  * No context call allocates device memory after ephmc_ctx_create, except:
  * the explicit ephmc_alloc; ephmc_ctx_set_checkpoint; the first call of the
- * reference algorithm (its Nt V^2 G_t buffers); and ephmc_leapfrog when it
- * meets more steps than before (its step log).  The static-disorder handle
+ * reference algorithm (its Nt V^2 G_t buffers); the first call of the mixed
+ * force (its segment buffers, about 3 Nt/C V^2 doubles, and a cuBLAS handle
+ * with a 32 MiB workspace), and again when a new segment length needs more;
+ * and ephmc_leapfrog when it meets more steps than before (its step log).  The static-disorder handle
  * grows its per-run buffers on demand, and ephmc_conv_* allocate per call.
  *
  * Errors: every ephmc_ function returns an ephmc_status; the most recent
@@ -79,7 +81,9 @@ typedef enum {
      * O(Nt) slice propagations instead of O(Nt log Nt), no G_t matrices. */
     EPHMC_FORCE_ADJOINT_FP64 = 1,
     /* Adjoint with FP64 M_hat, LU and log det, and FP32 propagation and
-     * contraction of the force (the mixed-precision MD force). */
+     * contraction of the force (the mixed-precision MD force), segmented:
+     * each segment's outer factor in FP64, the in-segment products in FP32
+     * (ephmc_ctx_set_segment). */
     EPHMC_FORCE_MIXED = 2
 } ephmc_force_mode;
 
@@ -186,6 +190,16 @@ EPHMC_API int ephmc_ctx_set_flags(ephmc_ctx *ctx, const ephmc_flags *flags);
  * interval 0 restores the whole stack.  The reference algorithm's G_t
  * buffers (Nt V^2 doubles) are separate and allocated on first use. */
 EPHMC_API int ephmc_ctx_set_checkpoint(ephmc_ctx *ctx, unsigned interval);
+/* No counterpart in the reference.  Segment length of the mixed force
+ * (EPHMC_FORCE_MIXED): the slice chain is cut into segments of `length`
+ * slices; each segment's G_t = L_t Z R_t takes its outer factor
+ * Z = Q_{t1-1} M^-1 P_{t0} in FP64 (sweep 1's state at the segment top, an
+ * FP64 y chain and one GEMM per segment) and only the in-segment products
+ * L_t, R_t in FP32, so the FP32 sums cancel over one segment's growth instead
+ * of the whole chain's.  0 restores the built-in length, min(Nt, 16).  With
+ * checkpointing (ephmc_ctx_set_checkpoint) the checkpoint interval is the
+ * segment length. */
+EPHMC_API int ephmc_ctx_set_segment(ephmc_ctx *ctx, unsigned length);
 /* No counterpart in the reference.  Chooses the launch shapes of the
  * thread-per-site sweeps (sites per thread, vectors per CTA) and the
  * dataflow LU's rows per thread for this context by timing each candidate

@@ -58,4 +58,5 @@ def test_force_matches_central_differences(gpu, restated):
     # measured 1.7e-5 and 8.5e-4.  The FD quotient itself is good to about
     # (rounding of log det ~ 2e-10) / (2 h) ~ 1e-6 absolute, 1.5e-5 of max |f|.
     assert err64 <= 1e-4
+    assert errm <= 1e-4
     assert errm <= 1e-2

@@ -67,7 +67,7 @@ def test_flag_variant_matches_reference(gpu, reference, restated, name, mode):
         assert err <= 1e-3
         return
     assert abs(ld - ld_r) <= 1e-12 * max(1.0, abs(ld_r))
-    assert err <= (2e-3 if mode == "mixed" else 1e-10)
+    assert err <= (1e-5 if mode == "mixed" else 1e-10)
 
 
 def test_zero_filling_force_is_ill_posed(restated):
