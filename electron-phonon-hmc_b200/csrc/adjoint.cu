@@ -231,12 +231,12 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     int T = (((V + S - 1) / S) + 31) / 32 * 32;
     const size_t per_vec = 9 * (size_t)V * sizeof(Real);
     const size_t fac_b = 3 * (size_t)V * sizeof(Real);
-    const size_t budget = 200 * 1024;
+    const size_t budget = 227 * 1024;  // the sm_100 per-block opt-in maximum
     int R = (int)((budget - fac_b) / per_vec);
     if (R < 1 || fac_b + per_vec > budget) {
         set_status(EPHMC_ERR_UNSUPPORTED, sizeof(Real) == 8
                                               ? "adjoint sweep: nine FP64 vectors of V sites exceed shared memory "
-                                                "(V > 2048); use the mixed or the reference force"
+                                                "(V > 2421); use the mixed or the reference force"
                                               : "adjoint sweep: nine FP32 vectors of V sites exceed shared memory");
         return EPHMC_ERR_UNSUPPORTED;
     }

@@ -346,9 +346,17 @@ unsigned seg_length(const ephmc_ctx *c) {
     return std::min(16u, std::max(1u, c->nt / 4));
 }
 
-SegPlan seg_plan(const ephmc_ctx *c) {
+// segments of the stabilised chain: shorter, since the accuracy of each
+// segment's Z_k falls with the conditioning of its middle product S_k (at
+// dtau = 0.31: 6 slices give 3e-6 of the largest force entry at 48x48,
+// beta = 40, against finite differences; 12 slices 3e-4)
+unsigned stab_seg_length(const ephmc_ctx *c) {
+    return std::min(c->seg_len ? c->seg_len : std::min(6u, std::max(1u, c->nt / 4)), c->nt);
+}
+
+SegPlan seg_plan(const ephmc_ctx *c, bool stab = false) {
     SegPlan p;
-    p.C = (int)seg_length(c);
+    p.C = (int)(stab ? stab_seg_length(c) : seg_length(c));
     p.b = ckpt_bounds(c->nt, (unsigned)p.C);
     p.m = (int)p.b.size() - 1;
     p.regions = c->ckpt == 0;
@@ -537,6 +545,107 @@ int force_mixed_seg(ephmc_ctx *c, const double *x, const double *y0, double logd
         rc = adjoint(1);
     }
     return rc;
+}
+
+// ------------------------------------------------------------------ stabilised evaluation
+// ephmc_ctx_set_stabilize: log det and the segments' y starts from the
+// UDT-stabilised chain (stabilize.cu), then the segment sweeps of the
+// adjoint (FP64) or mixed (FP32) force over the same segments.  The stacks
+// come from the identity at each segment's top (no sweep 1): all segments
+// in one launch (regions) or one at a time in one region (checkpointed).
+bool stab_applies(const ephmc_ctx *c, int mode) {
+    const ephmc_flags &f = c->flags;
+    return c->stabilize && mode != EPHMC_FORCE_REFERENCE && !f.constant_force && !f.single_particle &&
+           !f.zero_filling && !f.schur_form_inv;
+}
+
+// Issues the stabilised evaluation on the context stream without a host
+// wait: log|det| and its sign go to the LU's device words (c->lu.diag[V],
+// [V+1], status 0 in c->lu.info), as the LU would leave them, so that
+// ephmc_leapfrog collects them the same way; with want_force, the force.
+int stab_issue(ephmc_ctx *c, const double *x, int mode, bool want_force) {
+    const SegPlan p = seg_plan(c, true);
+    const int V = (int)c->V;
+    const size_t VV = (size_t)V * V;
+    const bool mixed = mode == EPHMC_FORCE_MIXED;
+    int rc;
+    if (3 * p.m > c->jobs_cap) return ret(EPHMC_ERR_ARG, "segment length too small for Nt");
+    if ((rc = stab_chain(c, &c->stab, x, p.b, want_force, c->jobs, 0))) return rc;
+    EPHMC_CUDA(cudaMemcpyAsync(c->lu.diag + V, stab_parts(c->stab), 2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                               c->stream));
+    EPHMC_CUDA(cudaMemsetAsync(c->lu.info, 0, 2 * sizeof(int), c->stream));
+    c->have_inverse = false;  // the stabilised chain forms no M_hat^-1
+    if (!want_force) return EPHMC_OK;
+    // segment stacks: regions in the q stack when it holds them, else in the chain's own buffer
+    const size_t esz = mixed ? sizeof(float) : sizeof(double);
+    const size_t need = esz * VV * (size_t)p.C * (p.regions ? (size_t)p.m : 1);
+    void *stack = c->qstack_bytes >= need ? c->qstack : stab_stack(c->stab, need);
+    if (!stack) return ret(EPHMC_ERR_NOMEM, "stabilised force: segment stacks");
+    std::vector<SliceJob> id;
+    for (int j = 0; j < p.m; ++j) {
+        const int t0 = p.b[j + 1], t1 = p.b[j];
+        SliceJob jb = job(nullptr, nullptr, t1 - 1, t1 - t0 - 1, -1, 0, kPairs, 1);
+        jb.stack = static_cast<char *>(stack) + (p.regions ? esz * VV * (size_t)j * p.C : 0);
+        jb.stack_off = -1 - t0;
+        id.push_back(jb);
+    }
+    if ((rc = upload_jobs(c, id, c->jobs + 2 * p.m))) return rc;
+    AdjointRange rg{0, 0, nullptr, nullptr, nullptr, true};
+    rg.seg_C = p.C;
+    rg.seg_regions = p.regions;
+    rg.y_start = stab_ystart(c->stab);
+    const double *none = nullptr;
+    auto adjoint = [&](int count) {
+        if (!mixed)
+            return launch_adjoint_sweep<double, double>(x, c->c, c->lat, static_cast<const double *>(stack), none,
+                                                        (int)c->nt, c->flavors, 0, 0.0, c->force, c->stream, &rg,
+                                                        count);
+        if (adjoint_strip_supported(c->lat))
+            return launch_adjoint_strip(x, c->c, c->lat, static_cast<const float *>(stack), none, (int)c->nt,
+                                        c->flavors, 0, 0.0, c->force, c->stream, &rg, count);
+        return launch_adjoint_sweep<float, float>(x, c->c, c->lat, static_cast<const float *>(stack), none, (int)c->nt,
+                                                  c->flavors, 0, 0.0, c->force, c->stream, &rg, count);
+    };
+    auto stacks = [&](int j0, int n) {
+        // segments of a single slice have no stack entries
+        int rc2 = EPHMC_OK;
+        for (int j = j0; j < j0 + n && rc2 == EPHMC_OK; ++j)
+            if (p.b[j] - p.b[j + 1] > 1) rc2 = launch_sweep1(c, x, c->jobs + 2 * p.m + j, mixed);
+        return rc2;
+    };
+    if (p.regions) {
+        // all segments' stacks in one launch when every segment has entries
+        bool all = true;
+        for (int j = 0; j < p.m; ++j) all = all && p.b[j] - p.b[j + 1] > 1;
+        rc = all ? launch_sweep1(c, x, c->jobs + 2 * p.m, mixed, p.m) : stacks(0, p.m);
+        rg.seg_j0 = 0;
+        if (rc == EPHMC_OK) rc = adjoint(p.m);
+    }
+    for (int j = p.m - 1; !p.regions && j >= 0 && rc == EPHMC_OK; --j) {
+        if ((rc = stacks(j, 1))) break;
+        rg.seg_j0 = j;
+        rg.zero_force = j == p.m - 1;
+        rg.y_start = stab_ystart(c->stab) + (size_t)j * VV;
+        rc = adjoint(1);
+    }
+    if (rc == EPHMC_OK && c->flags.no_fourier_acc)
+        rc = launch_boson_force(x, c->force, c->omega, 3 * V, (int)c->nt, false, c->stream);
+    return rc;
+}
+
+int stab_eval(ephmc_ctx *c, const double *x, int mode, bool want_force, double *logdet, int *sign) {
+    int rc = stab_issue(c, x, mode, want_force);
+    if (rc) return rc;
+    double parts[2] = {0, 1};
+    EPHMC_CUDA(cudaMemcpyAsync(parts, c->lu.diag + c->V, sizeof(parts), cudaMemcpyDeviceToHost, c->stream));
+    EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+    *logdet = parts[0];
+    *sign = parts[1] < 0 ? -1 : 1;
+    c->last_logdet = parts[0];
+    c->last_sign = *sign;
+    if (*sign < 0 && (c->flavors % 2)) add_warning(EPHMC_WARN_NEGATIVE_DET);
+    if (!std::isfinite(parts[0])) return ret(EPHMC_ERR_NONFINITE, "stabilised log det not finite");
+    return EPHMC_OK;
 }
 
 // M_hat (or, with a stack, sweep 1 of the adjoint) into dst (default c->M)
@@ -787,6 +896,7 @@ int ephmc::ensure_seg_buffers(ephmc_ctx *c) { return ensure_seg(c, seg_plan(c));
 int ephmc::eval_async(ephmc_ctx *c, const double *xd, int mode) {
     if (c->flags.single_particle || c->flags.schur_form_inv)
         return ret(EPHMC_ERR_UNSUPPORTED, "eval_async: the force needs the log det on the host");
+    if (stab_applies(c, mode)) return stab_issue(c, xd, mode, true);
     const bool adj = mode != EPHMC_FORCE_REFERENCE && !c->flags.constant_force;
     int rc;
     if ((rc = build_M_hat(c, xd, adj ? c->qstack : nullptr, mode == EPHMC_FORCE_MIXED))) return rc;
@@ -889,6 +999,7 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     lu_free(c->lu);
     schur_free(c->schur);
     if (c->seg) cudaFree(c->seg);
+    stab_free(c->stab);
     if (c->blas) cublasDestroy(static_cast<cublasHandle_t>(c->blas));
     if (c->blas_ws) cudaFree(c->blas_ws);
     if (c->batch_stream) cudaStreamDestroy(c->batch_stream);
@@ -1041,6 +1152,14 @@ int ephmc_ctx_set_checkpoint(ephmc_ctx *c, unsigned interval) {
     return EPHMC_OK;
 }
 
+int ephmc_ctx_set_stabilize(ephmc_ctx *c, int on) {
+    clear_status();
+    if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_stabilize");
+    ++c->param_gen;
+    c->stabilize = on != 0;
+    return EPHMC_OK;
+}
+
 int ephmc_ctx_set_segment(ephmc_ctx *c, unsigned length) {
     clear_status();
     if (!c) return ret(EPHMC_ERR_ARG, "ephmc_ctx_set_segment");
@@ -1179,6 +1298,7 @@ int ephmc_ctx_memory(const ephmc_ctx *c, size_t *bytes) {
     if (c->A) b += 2 * sizeof(double) * VV * c->refine_batch;
     b += sizeof(double) * VV + sizeof(int) * ((size_t)c->V + lu_sync_words((int)c->V));  // LU panel store, pivots
     b += c->seg_bytes + (c->blas_ws ? kBlasWorkspace : 0);  // segmented mixed force
+    b += stab_bytes(c->stab);                               // stabilised chain
     *bytes = b;
     return EPHMC_OK;
 }
@@ -1263,6 +1383,19 @@ int ephmc_eval(ephmc_ctx *c, const double *x, double *p_dot, double *logdet, int
     int rc;
     if ((rc = stage_in(c, x, c->x, dim, &xd))) return ret(rc);
     EPHMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    if (stab_applies(c, mode)) {
+        double ld = 0;
+        int sg = 1;
+        rc = stab_eval(c, xd, mode, p_dot != nullptr, &ld, &sg);
+        if (logdet) *logdet = ld;
+        if (rc) return ret(rc);
+        EPHMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
+        if ((rc = stage_out(c, p_dot, c->force, dim))) return ret(rc);
+        EPHMC_CUDA(cudaStreamSynchronize(c->stream));
+        cudaEventElapsedTime(&c->t_force, c->ev[0], c->ev[3]);
+        c->t_mhat = c->t_lu = 0;
+        return EPHMC_OK;
+    }
     const bool adj = mode != EPHMC_FORCE_REFERENCE && !f.constant_force;
     const bool mixed = mode == EPHMC_FORCE_MIXED;
     if ((rc = build_M_hat(c, xd, adj ? c->qstack : nullptr, mixed))) return ret(rc);

@@ -106,6 +106,20 @@ int schur_check(SchurSolver **slot, const double *M, int V, double *scratch, cud
 int launch_one_minus(double *G, const double *M, int V, cudaStream_t st);
 int launch_schur_clamp(double *force, size_t n, const double kappa[3], double f, cudaStream_t st);
 
+// ---------------------------------------------------------------- stabilised chain (stabilize.cu)
+struct StabWork;
+void stab_free(StabWork *w);
+size_t stab_bytes(const StabWork *w);
+// UDT-stabilised chain of the field x over the segments b (top down): log det
+// parts into stab_parts() (device: log|det M_hat|, sign), and with want_z each
+// segment's y start Z_j (row-major, top-down j, contiguous from stab_ystart()).
+// Uses 2m job slots from slot0 of the context's job table.
+int stab_chain(ephmc_ctx *c, StabWork **slot, const double *x, const std::vector<int> &b, bool want_z,
+               SliceJob *jobs_dev, int slot0);
+double *stab_ystart(StabWork *w);
+double *stab_parts(StabWork *w);
+void *stab_stack(StabWork *w, size_t bytes);  // segment stacks, grown on demand
+
 // ---------------------------------------------------------------- static disorder (trans_loc.cu)
 int tl_create_nnt(ephmc_tl **out, const unsigned *nnt, unsigned V, unsigned nbins, const double t[3],
                   const double kappa[3], double mu, const double contr_mat[6], unsigned lanes, int device);
@@ -332,6 +346,8 @@ struct ephmc_ctx {
     // chain at the segment starts and the segments' y starts, allocated on
     // first use; the cuBLAS handle of its Z GEMMs and that handle's workspace
     unsigned seg_len = 0;       // ephmc_ctx_set_segment (0: the built-in rule)
+    bool stabilize = false;     // ephmc_ctx_set_stabilize: UDT-stabilised chain (stabilize.cu)
+    ephmc::StabWork *stab = nullptr;
     double *seg = nullptr;
     size_t seg_bytes = 0;
     void *blas = nullptr;       // cublasHandle_t

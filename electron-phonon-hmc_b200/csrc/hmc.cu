@@ -387,6 +387,12 @@ int ephmc_leapfrog_graph(ephmc_ctx *c, double *x, double *p, unsigned steps, dou
     clear_status();
     int rc = leapfrog_prepare(c, x, p, steps, force_mode);
     if (rc) return rc;
+    if (c->stabilize && force_mode != EPHMC_FORCE_REFERENCE && !c->flags.constant_force) {
+        set_status(EPHMC_ERR_UNSUPPORTED,
+                   "ephmc_leapfrog_graph: the stabilised chain's cuSOLVER factorisations are not captured; use "
+                   "ephmc_leapfrog");
+        return EPHMC_ERR_UNSUPPORTED;
+    }
     if (force_mode == EPHMC_FORCE_REFERENCE || c->flags.constant_force)
         if ((rc = ensure_ref_buffers(c))) return rc;
     if (force_mode == EPHMC_FORCE_MIXED && !c->flags.constant_force)

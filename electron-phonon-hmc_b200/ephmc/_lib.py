@@ -75,6 +75,7 @@ def load_library(path: str | None = None, build_if_missing: bool = True):
     sig("ephmc_ctx_set_flags", _I, [_P, _P])
     sig("ephmc_ctx_set_checkpoint", _I, [_P, _U])
     sig("ephmc_ctx_set_segment", _I, [_P, _U])
+    sig("ephmc_ctx_set_stabilize", _I, [_P, _I])
     sig("ephmc_ctx_memory", _I, [_P, C.POINTER(C.c_size_t)])
     sig("ephmc_ctx_autotune", _I, [_P, _P, _I, C.POINTER(C.c_float), C.POINTER(C.c_float)])
     sig("ephmc_ctx_tuning", _I, [_P, C.POINTER(C.c_int)])

@@ -154,6 +154,17 @@ class Context:
         """Segment length of the mixed force (0: the built-in min(Nt, 16))."""
         check(self.lib.ephmc_ctx_set_segment(self.h, int(length)), "ephmc_ctx_set_segment")
 
+    def set_stabilize(self, on=True):
+        """FP64 re-stabilised slice chain for the adjoint and mixed paths."""
+        check(self.lib.ephmc_ctx_set_stabilize(self.h, int(bool(on))), "ephmc_ctx_set_stabilize")
+
+    def logdet(self, x, mode="adjoint"):
+        """log|det M_hat| alone (ephmc_eval without a force output)."""
+        m = MODES[mode] if isinstance(mode, str) else int(mode)
+        ld = C.c_double(0.0)
+        check(self.lib.ephmc_eval(self.h, ptr(x), None, C.byref(ld), m), "ephmc_eval")
+        return ld.value
+
     def set_checkpoint(self, interval):
         """Checkpointed adjoint sweeps every `interval` slices (0: whole stack)."""
         check(self.lib.ephmc_ctx_set_checkpoint(self.h, int(interval)), "ephmc_ctx_set_checkpoint")

@@ -200,6 +200,22 @@ EPHMC_API int ephmc_ctx_set_checkpoint(ephmc_ctx *ctx, unsigned interval);
  * checkpointing (ephmc_ctx_set_checkpoint) the checkpoint interval is the
  * segment length. */
 EPHMC_API int ephmc_ctx_set_segment(ephmc_ctx *ctx, unsigned length);
+/* No counterpart in the reference.  on != 0: the adjoint and mixed forces
+ * (and their log det) come from an FP64 re-stabilised slice chain, for low
+ * temperatures where the raw product 1 + B_0...B_{Nt-1} that the reference
+ * factors (simulation/organic_dense_matrix.c:251-265, :547-607) loses log det
+ * to rounding (at 48x48, Nt = 128, beta = 40 its LU resolves log det only to
+ * about 4e-6).  The partial products over the segments (ephmc_ctx_set_segment)
+ * are kept as U diag(d) T (QR with columns sorted by norm at every segment
+ * boundary); log det comes from a well-conditioned matrix N_0 and the
+ * segments' outer factors Z_k from N_k, and the segment sweeps run as in the
+ * unstabilised segmented force.  Costs about 17 V^3 flops per segment
+ * (cuSOLVER geqrf/orgqr/getrf/getrs, cuBLAS GEMM/trsm) on top of the sweeps.
+ * No M_hat^-1 is formed (ephmc_ctx_get_inverse then reports none).  Ignored
+ * by the reference force and by CONSTANT_FORCE, SINGLE_PARTICLE, ZERO_FILLING
+ * and SCHUR_FORM_INV contexts.  ephmc_eval with p_dot NULL computes the log
+ * det only (one chain of QR steps). */
+EPHMC_API int ephmc_ctx_set_stabilize(ephmc_ctx *ctx, int on);
 /* No counterpart in the reference.  Chooses the launch shapes of the
  * thread-per-site sweeps (sites per thread, vectors per CTA) and the
  * dataflow LU's rows per thread for this context by timing each candidate
