@@ -569,12 +569,20 @@ unsigned ephmc_run_hmc_seeded(unsigned long long seed, double *greens, unsigned 
 }
 
 // run_hmc (simulation/organic_hmc.c:296-353), seeded with time(NULL) as the
-// reference, or with the value of the environment variable EPHMC_SEED if set
+// reference, or with the value of the environment variable EPHMC_SEED if set.
+// EPHMC_FORCE (reference, adjoint or mixed) selects the force algorithm of a
+// host program that cannot call ephmc_set_dropin_force_mode itself, such as
+// the reference's unchanged organic_main; the default is the reference's.
 unsigned run_hmc(double *greens, unsigned l1, unsigned l2, unsigned nt, double *t, double *kappa, double mu,
                  double omega, unsigned flavors, double *contr_mat, unsigned steps, double traj_length, unsigned therm,
                  unsigned meas, unsigned meas_freq, const char *res_name, const char *corr_name, organic_flags *mode) {
     unsigned long long seed = (unsigned long long)std::time(nullptr);
     if (const char *s = std::getenv("EPHMC_SEED")) seed = std::strtoull(s, nullptr, 10);
+    if (const char *f = std::getenv("EPHMC_FORCE")) {
+        if (!std::strcmp(f, "reference")) ephmc_set_dropin_force_mode(EPHMC_FORCE_REFERENCE);
+        else if (!std::strcmp(f, "adjoint")) ephmc_set_dropin_force_mode(EPHMC_FORCE_ADJOINT_FP64);
+        else if (!std::strcmp(f, "mixed")) ephmc_set_dropin_force_mode(EPHMC_FORCE_MIXED);
+    }
     return ephmc_run_hmc_seeded(seed, greens, l1, l2, nt, t, kappa, mu, omega,
                                 flavors, contr_mat, steps, traj_length, therm, meas, meas_freq, res_name, corr_name,
                                 mode);
