@@ -6,9 +6,11 @@
 //   g_ab(tau) = sum_{i,j} chi_ia(0) chi_jb(tau) [ R_t0[j][i] R_0t[jb][ia] + R_t0[jb][ia] R_0t[j][i]
 //                                            - R_t0[jb][i] R_0t[j][ia] - R_t0[j][ia] R_0t[jb][i] ]
 //   greens[tau][a][b] = g / ns   (single particle: g e^{-logdet})
-// Both chains are single launches of the slice kernel with a spill stack
-// (all Nt matrices kept, 2 Nt V^2 doubles); the Wick contraction of all slices
-// is one launch over (j, tau) with the 9 (a,b) sums reduced per block.
+// R_t0 is one launch of the slice kernel that keeps every state (the caller's
+// Nt V^2 buffer, as the reference's R_t0); R_0t is a single V x V matrix that
+// advances one slice after each tau's contraction, as in the reference, so
+// no second Nt V^2 stack is held.  Each tau's Wick contraction is one launch
+// over j with the 9 (a,b) sums reduced per block.
 #include "ephmc_internal.cuh"
 
 namespace ephmc {
@@ -16,12 +18,12 @@ namespace ephmc {
 namespace {
 
 __global__ void k_cc_contract(const double *__restrict__ x, Couplings c, const int *__restrict__ nbr,
-                              const double *__restrict__ Rt0, const double *__restrict__ R0t, int V,
+                              const double *__restrict__ Rt0, const double *__restrict__ R0t, int V, int tau,
                               double *__restrict__ part) {
-    const int j = blockIdx.x, tau = blockIdx.y;
+    const int j = blockIdx.x;
     const size_t VV = (size_t)V * V;
     const double *A = Rt0 + (size_t)tau * VV;  // R_t0 at tau
-    const double *B = R0t + (size_t)tau * VV;  // R_0t at tau
+    const double *B = R0t;                     // R_0t at tau
     const double *x0 = x, *xt = x + (size_t)tau * 3 * V;
     double acc[9];
 #pragma unroll
@@ -79,7 +81,7 @@ int cc_correlator_dev(ephmc_ctx *c, const double *x, const double *Minv, double 
     const size_t VV = (size_t)V * V;
     cudaStream_t st = c->stream;
     const bool plain = !(c->flags.zero_filling || c->flags.single_particle);
-    double *start_t0 = c->work, *start_0t = R_0t;  // R_0t: a chain of nt matrices
+    double *start_t0 = c->work, *start_0t = R_0t;  // R_0t: one matrix, advanced slice by slice
     int rc;
     if (plain) {
         if ((rc = launch_copy(start_t0, Minv, VV, st))) return rc;
@@ -101,24 +103,29 @@ int cc_correlator_dev(ephmc_ctx *c, const double *x, const double *Minv, double 
     j1.p_begin = 0;
     j1.p_end = kPairs;
     j1.p_step = 1;
-    // R_0t chain: slices 0 .. Nt-2 applied to rows, state after slice tau kept at R_0t[tau+1]
-    SliceJob j2 = j1;
-    j2.src = start_0t;
-    j2.dst = R_0t + (size_t)(nt - 1) * VV;
-    j2.stack = R_0t;
-    j2.stack_off = 1;
-    j2.s_first = 0;
-    j2.s_count = nt - 1;
-    j2.s_dir = 1;
-    SliceJob jobs[2] = {j1, j2};
-    if ((rc = ctx_upload_jobs(c, jobs, 2, 0, st))) return rc;
+    // R_0t: slice tau applied to the rows in place after tau's contraction
+    std::vector<SliceJob> jobs{j1};
+    for (int tau = 0; tau + 1 < nt; ++tau) {
+        SliceJob j2 = j1;
+        j2.src = R_0t;
+        j2.dst = R_0t;
+        j2.stack = nullptr;
+        j2.s_first = tau;
+        j2.s_count = 1;
+        j2.s_dir = 1;
+        jobs.push_back(j2);
+    }
+    if ((rc = ctx_upload_jobs(c, jobs.data(), (int)jobs.size(), 0, st))) return rc;
     if ((rc = launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs, 1, st))) return rc;
-    if (nt > 1)
-        if ((rc = launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs + 1, 1, st))) return rc;
     double *part = c->cc_part;  // nt * V * 9 doubles
-    k_cc_contract<<<dim3(V, nt), 256, 0, st>>>(x, c->c, c->lat.nbr, R_t0, R_0t, V, part);
-    count_launch(1);
-    EPHMC_CUDA(cudaGetLastError());
+    for (int tau = 0; tau < nt; ++tau) {
+        k_cc_contract<<<V, 256, 0, st>>>(x, c->c, c->lat.nbr, R_t0, R_0t, V, tau, part);
+        count_launch(1);
+        EPHMC_CUDA(cudaGetLastError());
+        if (tau + 1 < nt &&
+            (rc = launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, c->jobs + 1 + tau, 1, st)))
+            return rc;
+    }
     const double scale = c->flags.single_particle ? std::exp(-logdet) : 1.0 / V;
     k_cc_final<<<(nt * 9 + 127) / 128, 128, 0, st>>>(part, V, nt, scale, greens);
     count_launch(1);

@@ -81,16 +81,6 @@ ephmc_ctx *ctx_for(unsigned *nnt, unsigned ns, unsigned nt, double *t, double *k
     return c;
 }
 
-// nt V^2 doubles for the correlator's R_0t chain: the q stack when it holds the
-// whole sweep, else the reference-algorithm G buffer (allocated on first use),
-// else `fallback`
-double *correlator_chain(ephmc_ctx *c, double *fallback) {
-    const size_t need = sizeof(double) * (size_t)c->nt * c->V * c->V;
-    if (c->qstack && c->qstack_bytes >= need) return static_cast<double *>(c->qstack);
-    if (ensure_ref_buffers(c) == EPHMC_OK) return c->G;
-    return fallback;
-}
-
 double logdet_dev(ephmc_ctx *c, double *M, unsigned ns, unsigned flavors) {
     double ld = 0;
     if (c->flags.single_particle) {
@@ -232,7 +222,7 @@ short trajectory_dev(ephmc_ctx *c, double *xb, double *results, double *greens, 
         if (greens) {
             double *gd = nullptr;
             cudaMalloc(&gd, sizeof(double) * nt * 9);
-            cc_correlator_dev(c, x, M_hat, QM1P, correlator_chain(c, QM1P), gd, logDetM);
+            cc_correlator_dev(c, x, M_hat, QM1P, c->work + (size_t)ns * ns, gd, logDetM);
             cudaMemcpy(greens, gd, sizeof(double) * nt * 9, cudaMemcpyDeviceToHost);
             cudaFree(gd);
             if (corr_out) {  // fprint_corr (simulation/organic_aux.c:51-60)
@@ -506,17 +496,17 @@ void cc_correlator(double *x, double *M_hat, double *R_t0, double *R_0t, double 
     if (!c) return;
     const size_t dim = (size_t)nt * ns * 3, VV = (size_t)ns * ns;
     Dev X(x, dim), Mi(M_hat, VV), Rt(R_t0, VV * nt, false), G(greens, (size_t)nt * 9, false);
-    double *chain = correlator_chain(c, nullptr);  // nt V^2 doubles
-    if (!chain || cc_correlator_dev(c, X.d, Mi.d, Rt.d, chain, G.d, logDetM) != EPHMC_OK) {
+    double *r0t = c->work + VV;  // R_0t on the device, advanced slice by slice
+    if (cc_correlator_dev(c, X.d, Mi.d, Rt.d, r0t, G.d, logDetM) != EPHMC_OK) {
         std::fprintf(stderr, "ephmc cc_correlator: %s\n", ephmc_last_error_message());
         return;
     }
     cudaStreamSynchronize(c->stream);
     if (R_0t) {  // the reference leaves R_0t after Nt-1 slices
         if (devp(R_0t))
-            cudaMemcpy(R_0t, chain + (size_t)(nt - 1) * VV, sizeof(double) * VV, cudaMemcpyDeviceToDevice);
+            cudaMemcpy(R_0t, r0t, sizeof(double) * VV, cudaMemcpyDeviceToDevice);
         else
-            cudaMemcpy(R_0t, chain + (size_t)(nt - 1) * VV, sizeof(double) * VV, cudaMemcpyDeviceToHost);
+            cudaMemcpy(R_0t, r0t, sizeof(double) * VV, cudaMemcpyDeviceToHost);
     }
     Rt.back();
     G.back();

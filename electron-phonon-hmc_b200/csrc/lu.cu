@@ -30,6 +30,8 @@
 // V = 1024, with no separate triangular-solve phase.
 #include "ephmc_internal.cuh"
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 
@@ -332,10 +334,16 @@ __device__ __forceinline__ bool warp_argmax_fast(unsigned long long &key, int &l
     return warp_argmax_lpos(k2, l2);
 }
 
-// 1/d by two Newton-Raphson steps x <- x + x (1 - d x) from the hardware
-// reciprocal approximation (PTX rcp.approx.ftz.f64); within one unit in the
-// last place of the correctly rounded quotient for normal d.
+// 1/d by Newton-Raphson iteration for the reciprocal, x <- x + x (1 - d x)
+// (the error e = 1 - d x squares at each step; the iteration as written for a
+// fused multiply-add in P. Markstein, IA-64 and Elementary Functions, 2000,
+// ch. 8), two steps from the hardware approximation of PTX rcp.approx.ftz.f64.
+// The approximation flushes subnormal arguments and results to zero, so for
+// |d| outside [2^-1021, 2^1021] (subnormal pivots, pivots whose reciprocal is
+// subnormal, zero, inf, NaN) the quotient 1.0 / d is taken instead.
 __device__ __forceinline__ double recip_nr(double d) {
+    const double a = fabs(d);
+    if (!(a >= 0x1p-1021 && a <= 0x1p1021)) return 1.0 / d;
     double x;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(d));
     double e = fma(-d, x, 1.0);
@@ -357,7 +365,7 @@ template <int NB, int RPT, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) k_gj_dataflow(double *__restrict__ M, int V,
                                                         double *__restrict__ panels, int *__restrict__ ipiv,
                                                         double *__restrict__ diag, int *__restrict__ info,
-                                                        unsigned *__restrict__ sync) {
+                                                        unsigned *__restrict__ sync, int withhold) {
     constexpr int MW = MAXT / 32;
     // per warp candidate of a pivot step: |value| key, logical position,
     // physical row, value, and the row already divided by its pivot entry
@@ -480,7 +488,8 @@ __global__ void __launch_bounds__(MAXT, 1) k_gj_dataflow(double *__restrict__ M,
                 for (int q = 0; q < NB; ++q)
                     if (row[i] < V && q < nbc) panels[(size_t)(j0 + q) * V + row[i]] = a[i][q];
             __syncthreads();
-            if (tid == 0) st_release_u32(ready + k, epoch);
+            // (withhold: test hook, the flag of that one panel is never set)
+            if (tid == 0 && k != withhold) st_release_u32(ready + k, epoch);
         } else {
             const int buf = k & 1;
             // one warp waits and fetches the panel's pivots; the next owner
@@ -664,6 +673,10 @@ int run_panels(double *M, LUWork &w, cudaStream_t st) {
     return EPHMC_OK;
 }
 
+// ephmc_test_lu_withhold_next: the panel whose ready flag the next dataflow
+// launch does not set (-1: none)
+std::atomic<int> g_lu_withhold{-1};
+
 template <int RPT, int MAXT>
 int launch_dataflow(double *M, LUWork &w, int nblk, int T, int sms, cudaStream_t st) {
     int per_sm = 0;
@@ -671,7 +684,8 @@ int launch_dataflow(double *M, LUWork &w, int nblk, int T, int sms, cudaStream_t
     if ((long)per_sm * sms < nblk) return EPHMC_ERR_UNSUPPORTED;
     const int V = w.V;
     double *panels = w.X;
-    void *args[] = {&M, (void *)&V, &panels, &w.ipiv, &w.diag, &w.info, &w.sync};
+    int withhold = g_lu_withhold.exchange(-1);  // one call only
+    void *args[] = {&M, (void *)&V, &panels, &w.ipiv, &w.diag, &w.info, &w.sync, &withhold};
     EPHMC_CUDA(cudaLaunchCooperativeKernel((const void *)k_gj_dataflow<kLuPanel, RPT, MAXT>, dim3(nblk), dim3(T), args,
                                            0, st));
     ephmc::count_launch(1);
@@ -796,3 +810,5 @@ int lu_logdet_inverse(double *M, LUWork &w, double *logdet, int *sign, int *ipiv
 }
 
 }  // namespace ephmc
+
+extern "C" EPHMC_API void ephmc_test_lu_withhold_next(int panel) { ephmc::g_lu_withhold.store(panel); }

@@ -17,12 +17,13 @@
 //    calls that overlap on the GPU (different streams or threads, or another
 //    device context sharing the GPU) race on it and must be serialised by the
 //    caller;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress, with that device current) and caches it; make
-//    that first call before any stream capture.
+//  * every call looks up the array's device address on the current device
+//    (cudaGetSymbolAddress, a host-side lookup), so no address outlives a
+//    device reset or belongs to another device;
+//  * the matrix must be memory of the current device;
+//  * the call synchronizes the stream before it returns: log|det|, the sign
+//    and the pivots are read back to the host.
 #include "ephmc_internal.cuh"
-
-#include <mutex>
 
 namespace {
 
@@ -39,25 +40,13 @@ constexpr size_t kNoAllocBytes = kOffSync + align256(sizeof(unsigned) * ephmc::l
 // stand-in); the device address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char *g_addr[kMaxDevices] = {nullptr};
-
+// the array's device address on the current device, looked up anew by every
+// call (a cached address would be stale after a device reset)
 int scratch_for_current_device(unsigned char **out) {
-    int dev = 0;
-    EPHMC_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) {
-        ephmc::set_status(EPHMC_ERR_UNSUPPORTED, "device ordinal beyond the no-alloc table");
-        return EPHMC_ERR_UNSUPPORTED;
-    }
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return ephmc::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_addr[dev] = static_cast<unsigned char *>(p);
-    }
-    *out = g_addr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return ephmc::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    *out = static_cast<unsigned char *>(p);
     return EPHMC_OK;
 }
 
@@ -84,6 +73,14 @@ EPHMC_API int ephmc_logdet_inverse_noalloc(double *M, unsigned n, double *logdet
         ephmc::set_status(EPHMC_ERR_ARG, "ephmc_logdet_inverse_noalloc: M must be device memory");
         return EPHMC_ERR_ARG;
     }
+    int dev = 0;
+    EPHMC_CUDA(cudaGetDevice(&dev));
+    if (a.type == cudaMemoryTypeDevice && a.device != dev) {
+        // the workspace of the current device would be combined with another GPU's matrix
+        ephmc::set_status(EPHMC_ERR_ARG, "ephmc_logdet_inverse_noalloc: M is memory of another device than the "
+                                         "current one");
+        return EPHMC_ERR_ARG;
+    }
     unsigned char *base = nullptr;
     int rc = scratch_for_current_device(&base);
     if (rc != EPHMC_OK) return rc;
@@ -97,15 +94,14 @@ EPHMC_API int ephmc_logdet_inverse_noalloc(double *M, unsigned n, double *logdet
     w.sync_words = ephmc::lu_sync_words(kNoAllocMaxN);
     int sg = 1;
     double ld = 0;
+    // synchronizes the stream: the results come back to the host
     rc = ephmc::lu_logdet_inverse(M, w, &ld, &sg, ipiv, static_cast<cudaStream_t>(stream));
-    if (logdet) *logdet = ld;
-    if (sign) *sign = sg;
     if (rc != EPHMC_OK) {
         ephmc::set_status(rc, rc == EPHMC_ERR_SINGULAR ? "zero pivot" : nullptr);
-        return rc;
+        return rc;  // *logdet and *sign are left as they were
     }
-    const cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
-    if (e != cudaSuccess) return ephmc::cuda_fail(e, "cudaStreamSynchronize");
+    if (logdet) *logdet = ld;
+    if (sign) *sign = sg;
     return EPHMC_OK;
 }
 

@@ -156,9 +156,11 @@ EPHMC_API int ephmc_logdet_inverse(ephmc_ctx *ctx, double *M, int *ipiv, double 
  * is a file-scope device array (about 0.5 MB, held by every GPU that loads the
  * library until exit), shared by all calls and left holding the last call's
  * data: calls that overlap on the GPU race and must be serialised by the
- * caller.  The first call on each device looks up the array's address and
- * should come before any stream capture.  n > 256 returns EPHMC_ERR_ARG.
- * ipiv (host, may be NULL) receives 1-based pivots; stream may be NULL. */
+ * caller.  Every call looks up the array's address on the current device, and
+ * M must be memory of that device (else EPHMC_ERR_ARG).  The call synchronizes
+ * the stream before it returns.  n > 256 returns EPHMC_ERR_ARG; on any failure
+ * *logdet and *sign are left unchanged.  ipiv (host, may be NULL) receives
+ * 1-based pivots; stream may be NULL. */
 EPHMC_API int ephmc_logdet_inverse_noalloc(double *M, unsigned n, double *logdet, int *sign, int *ipiv,
                                            void *stream);
 
@@ -362,6 +364,13 @@ EPHMC_API unsigned long long ephmc_launch_count(void);
  * else FP32), from a dependent-chain FMA probe; the roofline denominator for
  * the stencil kernels. */
 EPHMC_API int ephmc_measure_fma_peak(int fp64, float *tflops);
+
+/* No counterpart in the reference.  Test hook of the LU's failure path: the
+ * next dataflow LU launch (V <= 1024) does not set the ready flag of panel
+ * `panel`, so the CTAs that wait for it give up after their bounded wait (2 s)
+ * and the call returns EPHMC_ERR_TIMEOUT, with the flags cleared for the next
+ * call.  -1 cancels.  Affects one launch only. */
+EPHMC_API void ephmc_test_lu_withhold_next(int panel);
 
 /* Library version string. */
 EPHMC_API const char *ephmc_version(void);

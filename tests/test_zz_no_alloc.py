@@ -81,3 +81,37 @@ def test_noalloc_alternating_sizes(gpu):
         inv = Md.cpu().numpy()
         ref = np.linalg.inv(A)
         assert np.max(np.abs(inv - ref)) <= 1e-10 * np.max(np.abs(ref)), n
+
+
+def test_noalloc_singular_then_regular(gpu):
+    """The all-ones matrix has an exact zero pivot at the second step:
+    EPHMC_ERR_SINGULAR, with *logdet and *sign left as they were; the next
+    call, of another size, on the same static workspace is correct."""
+    import torch
+    lib = _lib()
+    Md = torch.ones((64, 64), dtype=torch.float64, device="cuda")
+    ld, sg = C.c_double(123.0), C.c_int(7)
+    st = lib.ephmc_logdet_inverse_noalloc(Md.data_ptr(), 64, C.byref(ld), C.byref(sg), None, None)
+    assert st == 4
+    assert ld.value == 123.0 and sg.value == 7
+    rng = np.random.default_rng(11)
+    A = rng.standard_normal((100, 100)) + 3.0 * np.eye(100)
+    Md = torch.from_numpy(A.copy()).cuda()
+    st, ld2, sg2, _ = _noalloc(lib, Md, 100)
+    assert st == 0, lib.ephmc_last_error_message()
+    s_np, ld_np = np.linalg.slogdet(A.T)
+    assert abs(ld2 - ld_np) <= 1e-11 * abs(ld_np) and sg2 == int(s_np)
+    assert np.max(np.abs(Md.cpu().numpy() - np.linalg.inv(A.T).T)) <= 1e-10 * np.max(np.abs(np.linalg.inv(A)))
+
+
+def test_noalloc_refuses_another_devices_matrix(gpu):
+    """A matrix on another GPU than the current one is refused (the static
+    workspace is per device); runs only where a second device exists."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one CUDA device")
+    lib = _lib()
+    Md = torch.eye(16, dtype=torch.float64, device="cuda:1")
+    torch.cuda.set_device(0)
+    st, _, _, _ = _noalloc(lib, Md, 16)
+    assert st == 2
