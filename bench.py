@@ -46,6 +46,7 @@ L, NT, BETA = 32, 64, 20.0
 J, LAM, MU0, OMEGA0 = (1.0, -0.5, -0.5), (0.3, 0.15, 0.15), -3.0, 0.05
 WORKLOAD = "32x32 triangular lattice (V=1024), Nt=64, beta=20, force+logdet eval"
 TRAJ_BETA = 10.0  # the timed trajectory (beta = 20 diverges in the MD, in the reference as well)
+DH_TRAJ = 20      # trajectories of the mixed-vs-FP64 dH comparison in the headline line
 
 # Algorithmic work of one evaluation (reference algorithm, Taylor-4 as two pairs):
 # FLOP = V^2 Nt (84 (1 + log2 Nt) + 170) + 2 V^3 ; per slice application 84 V^2 flop.
@@ -58,6 +59,14 @@ ADJ_SWEEP_FLOP = 173 * V * V * NT
 SWEEP1_FLOP = 84 * V * V * NT
 # LU + inverse (getrf + getri): 2 V^3
 LU_FLOP = 2 * V ** 3
+# the segmented mixed force (segments of 16 slices, m = Nt/16): the M_hat phase
+# is sweep 1 plus the FP32 stacks of segments 1..m-1 from the identity
+# (C - 1 slices each); the force phase is the FP64 y chain (Nt - C slices),
+# m - 1 DGEMMs of 2 V^3 for the segments' start rows, and the FP32 sweep
+SEG_C = 16
+SEG_M = NT // SEG_C
+MIXED_MHAT_FLOP = 84 * V * V * (NT + (SEG_M - 1) * (SEG_C - 1))
+MIXED_FORCE_FLOP = 84 * V * V * (NT - SEG_C) + 2 * V ** 3 * (SEG_M - 1) + ADJ_SWEEP_FLOP
 
 
 # static-disorder workload: input.txt units, converted as organic_main does with
@@ -124,79 +133,12 @@ def run_batch_bench(args):
     import ephmc
     lib = ephmc.load_library()
     chains = batch_chains()
-    W, K = max(3, args.warmup), max(1, args.steps)
-    ctxs, xs, pds = [], [], []
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(77 + rank)
-    for L, nt, beta, s in chains:
-        t, kappa, mu, omega = ephmc.convert_params(beta, nt, J, tuple(s * v for v in LAM), MU0, OMEGA0)
-        c = ephmc.Context(L, L, nt, t, kappa, mu, omega, device=local)
-        ctxs.append(c)
-        xs.append(torch.randn(c.dim, dtype=torch.float64, device=dev, generator=gen))
-        pds.append(torch.empty(c.dim, dtype=torch.float64, device=dev))
-
-    def run_batch(x, p):
-        try:
-            ephmc.batch_eval(ctxs, x, p, mode="mixed")
-        except ephmc.EphmcError as e:  # chains outside the Taylor regime may give a non-finite log det
-            if e.status != 5:
-                raise
-
-    def run_seq():
-        for c, x, p in zip(ctxs, xs, pds):
-            try:
-                c.eval(x, p, mode="mixed")
-            except ephmc.EphmcError as e:
-                if e.status != 5:
-                    raise
-
-    # launch shapes per chain, by measurement (ephmc_ctx_autotune), before any timing
-    tune_gain = []
-    for c, x in zip(ctxs, xs):
-        try:
-            b, a, _ = c.autotune(x, "mixed")
-            tune_gain.append((b, a))
-        except ephmc.EphmcError as e:
-            if e.status != 5:
-                raise
-    for _ in range(W):
-        run_batch(xs, pds)
-    run_seq()
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    launches0 = lib.ephmc_launch_count()
-    with ClockSampler(local) as sampler:
-        t0 = time.perf_counter()
-        for _ in range(K):
-            run_batch(xs, pds)
-        torch.cuda.synchronize()
-        batch_s = time.perf_counter() - t0
-    launches = lib.ephmc_launch_count() - launches0
-    t0 = time.perf_counter()
-    for _ in range(K):
-        run_seq()
-    torch.cuda.synchronize()
-    seq_s = time.perf_counter() - t0
-    batch_s = max_over_ranks(batch_s, dist, dev)
-    seq_s = max_over_ranks(seq_s, dist, dev)
+    W, K = max(3, args.warmup), max(1, min(args.steps, 50))
+    res = batch_measure(lib, dev, local, chains, W, K, dist, tune=True)
+    ctxs, batch_s, seq_s, launches, sampler, tune_gain, e2e = (res[k] for k in (
+        "ctxs", "batch_s", "seq_s", "launches", "sampler", "tune_gain", "e2e"))
     n = len(ctxs)
     value = ws * K * n / batch_s
-    # e2e: host fields and forces (pinned) through the C ABI
-    xh = [torch.empty(c.dim, dtype=torch.float64, pin_memory=True) for c in ctxs]
-    ph = [torch.empty(c.dim, dtype=torch.float64, pin_memory=True) for c in ctxs]
-    for a, b in zip(xh, xs):
-        a.copy_(b.cpu())
-    xnp, pnp = [a.numpy() for a in xh], [a.numpy() for a in ph]
-    run_batch(xnp, pnp)
-    if dist is not None:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(K):
-        run_batch(xnp, pnp)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
-    nbytes = sum(8 * c.dim for c in ctxs)
-    e2e = {"value": ws * K * n / e2e_s, "unit": BATCH_UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
     if rank == 0:
         fp64 = C_float_peak(lib, True)
         flop = batch_flop(chains)
@@ -234,6 +176,92 @@ def run_batch_bench(args):
     return 0
 
 
+def batch_measure(lib, dev, local, chains, W, K, dist, tune=True):
+    """The 64-chain batch: contexts and N(0,1) fields on the device, optional
+    per-chain autotuning, W warm-up and K timed batches (ephmc_batch_eval),
+    the same chains one at a time, and the batch through the C ABI with host
+    buffers.  Returns the timings and the contexts (the caller closes them)."""
+    import torch
+
+    import ephmc
+    ws, rank, _ = dist_env()
+    ctxs, xs, pds = [], [], []
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(77 + rank)
+    for L, nt, beta, s in chains:
+        t, kappa, mu, omega = ephmc.convert_params(beta, nt, J, tuple(s * v for v in LAM), MU0, OMEGA0)
+        c = ephmc.Context(L, L, nt, t, kappa, mu, omega, device=local)
+        ctxs.append(c)
+        xs.append(torch.randn(c.dim, dtype=torch.float64, device=dev, generator=gen))
+        pds.append(torch.empty(c.dim, dtype=torch.float64, device=dev))
+
+    def run_batch(x, p):
+        try:
+            ephmc.batch_eval(ctxs, x, p, mode="mixed")
+        except ephmc.EphmcError as e:  # chains outside the Taylor regime may give a non-finite log det
+            if e.status != 5:
+                raise
+
+    def run_seq():
+        for c, x, p in zip(ctxs, xs, pds):
+            try:
+                c.eval(x, p, mode="mixed")
+            except ephmc.EphmcError as e:
+                if e.status != 5:
+                    raise
+
+    # launch shapes per chain, by measurement (ephmc_ctx_autotune), before any timing
+    tune_gain = []
+    for c, x in zip(ctxs, xs):
+        if not tune:
+            break
+        try:
+            b, a, _ = c.autotune(x, "mixed")
+            tune_gain.append((b, a))
+        except ephmc.EphmcError as e:
+            if e.status != 5:
+                raise
+    for _ in range(W):
+        run_batch(xs, pds)
+    run_seq()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches0 = lib.ephmc_launch_count()
+    with clock_sampler(local) as sampler:
+        t0 = time.perf_counter()
+        for _ in range(K):
+            run_batch(xs, pds)
+        torch.cuda.synchronize()
+        batch_s = time.perf_counter() - t0
+    launches = lib.ephmc_launch_count() - launches0
+    t0 = time.perf_counter()
+    for _ in range(K):
+        run_seq()
+    torch.cuda.synchronize()
+    seq_s = time.perf_counter() - t0
+    batch_s = max_over_ranks(batch_s, dist, dev)
+    seq_s = max_over_ranks(seq_s, dist, dev)
+    n = len(ctxs)
+    # e2e: host fields and forces (pinned) through the C ABI
+    xh = [torch.empty(c.dim, dtype=torch.float64, pin_memory=True) for c in ctxs]
+    ph = [torch.empty(c.dim, dtype=torch.float64, pin_memory=True) for c in ctxs]
+    for a, b in zip(xh, xs):
+        a.copy_(b.cpu())
+    xnp, pnp = [a.numpy() for a in xh], [a.numpy() for a in ph]
+    run_batch(xnp, pnp)
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        run_batch(xnp, pnp)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    nbytes = sum(8 * c.dim for c in ctxs)
+    e2e = {"value": ws * K * n / e2e_s, "unit": BATCH_UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+    return {"ctxs": ctxs, "batch_s": batch_s, "seq_s": seq_s, "launches": launches, "sampler": sampler,
+            "tune_gain": tune_gain, "e2e": e2e}
+
+
 def batch_cpu_baseline(chains, budget=60.0):
     """The reference (oracle/_ref) on the host: one evaluation of each chain in
     turn until all are done or `budget` seconds have passed."""
@@ -262,6 +290,61 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
+
+
+class NvmlClockSampler:
+    """SM clocks and throttle reasons during the timed region, polled in-process
+    through NVML every 20 ms (a one-sample nvidia-smi record of a sub-second
+    region says little)."""
+
+    def __init__(self, index):
+        import pynvml
+        self.nv = pynvml
+        self.BITS = {"hw_slowdown": pynvml.nvmlClocksThrottleReasonHwSlowdown,
+                     "sw_thermal_slowdown": pynvml.nvmlClocksThrottleReasonSwThermalSlowdown,
+                     "hw_thermal_slowdown": pynvml.nvmlClocksThrottleReasonHwThermalSlowdown,
+                     "sw_power_cap": pynvml.nvmlClocksThrottleReasonSwPowerCap}
+        pynvml.nvmlInit()
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+        self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                self.samples.append((mhz, reasons))
+            except Exception:
+                pass
+            self._stop.wait(0.02)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["NVML returned no sample"], "samples": 0}
+        reasons = sorted({n for _, r in self.samples for n, bit in self.BITS.items() if r & bit})
+        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "NVML, every 20 ms"}
+
+
+def clock_sampler(index):
+    try:
+        return NvmlClockSampler(index)
+    except Exception:
+        return ClockSampler(index)
 
 
 class ClockSampler:
@@ -560,10 +643,11 @@ def load_ncu_summary():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-chain batch field of the headline line")
     ap.add_argument("--paths", default="mixed,adjoint,reference")
     ap.add_argument("--profile", action="store_true",
                     help="run only warm-up + timed evaluations of --paths (for ncu); print nothing")
@@ -631,7 +715,7 @@ def main():
         launches0 = lib.ephmc_launch_count()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
         ph = []
-        sampler = ClockSampler(local) if path == "mixed" else None
+        sampler = clock_sampler(local) if path == "mixed" else None
         if sampler:
             sampler.__enter__()
         for k in range(K):
@@ -678,36 +762,102 @@ def main():
     e2e = {"value": whole_job_rate(ws, K, e2e_s), "unit": UNIT, "h2d_bytes_per_step": 8 * dim,
            "d2h_bytes_per_step": 8 * dim + 8}
 
-    # one HMC trajectory's device work: Nmd = 20 leapfrog steps with Fourier
-    # acceleration over traj_length = pi/2 (ephmc_leapfrog), then the accept
-    # step's evaluation, from a free-phonon field (run_hmc's start,
-    # simulation/organic_hmc.c:325) and accelerated momenta.  At beta = 20 the
-    # molecular dynamics diverges within two steps, in the reference's own HMC
-    # as here (acceptance 0, e^-dH NaN on 8x8, Nt = 64); the trajectory is timed
-    # on the same lattice and Nt at beta = 10, where it accepts.
+    # One whole HMC trajectory (trajectory, simulation/organic_hmc.c:192-294,
+    # without the measurement rows): momenta drawn N(0,1) on the device and
+    # Fourier-accelerated (sample_fourier_momenta), their energy and the
+    # action, Nmd = 20 leapfrog steps with Fourier acceleration over pi/2
+    # (ephmc_leapfrog), the accept-step evaluation with its FP64 log det, the
+    # new action and the Metropolis decision on the host; wall clock per
+    # trajectory.  beta = 10: at beta = 20 the molecular dynamics diverges
+    # within two steps, in the reference's own HMC as here (acceptance 0,
+    # e^-dH NaN on 8x8, Nt = 64).
     tt, tk, tmu, tom = ephmc.convert_params(TRAJ_BETA, NT, J, LAM, MU0, OMEGA0)
     tctx = ephmc.Context(L, L, NT, tt, tk, tmu, tom, device=local)
     lib.ephmc_ctx_set_stream(tctx.h, stream.cuda_stream)
+    urng = np.random.default_rng(4321 + rank)
+
+    def hmc_trajectory(c, x, ld_x, mode):
+        p0 = torch.randn(dim, dtype=torch.float64, device=dev, generator=gen)
+        c.fa_scale_momenta(p0)
+        h0 = c.hamilton(x, ld_x, c.fa_energy(p0))
+        x1 = x.clone()
+        c.leapfrog(x1, p0, 20, float(np.pi / 2), mode)
+        ld1, _ = c.eval(x1, pd, mode=mode)
+        dh = c.hamilton(x1, ld1, c.fa_energy(p0)) - h0
+        accept = urng.random() < np.exp(-dh)
+        return (x1, ld1, dh, accept) if accept else (x, ld_x, dh, accept)
+
     xt = torch.randn(dim, dtype=torch.float64, device=dev, generator=gen)
     tctx.fa_scale_free_bosons(xt)
-    traj_ms, traj_fail = [], None
-    for k in range(5):
-        pt = torch.randn(dim, dtype=torch.float64, device=dev, generator=gen)
-        tctx.fa_scale_momenta(pt)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        try:
-            tctx.leapfrog(xt, pt, 20, float(np.pi / 2), head)
-            tctx.eval(xt, pd, mode=head)
-        except ephmc.EphmcError as e:
-            traj_fail = str(e)
-            break
-        e1.record(stream)
-        torch.cuda.synchronize()
-        if k >= 2:
-            traj_ms.append(e0.elapsed_time(e1))
+    traj_ms, traj_fail, traj_acc = [], None, []
+    try:
+        ldt, _ = tctx.eval(xt, pd, mode=head)
+        for k in range(12):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            xt, ldt, _, acc = hmc_trajectory(tctx, xt, ldt, head)
+            torch.cuda.synchronize()
+            if k >= 2:
+                traj_ms.append(1e3 * (time.perf_counter() - t0))
+                traj_acc.append(acc)
+    except ephmc.EphmcError as e:
+        traj_fail = str(e)
     tctx.close()
     traj = max_over_ranks(statistics.median(traj_ms), dist, dev) if traj_ms else None
+
+    # The mixed force's Hamiltonian error: trajectories from the same field and
+    # momenta with the FP64 adjoint force and with the mixed force, at beta = 10
+    # and mu0 = 0 (with the band empty at mu0 = -3 the fermion force hardly
+    # enters dH; at mu0 = 0 |dH| ~ 1e-2); the chain follows the FP64 run.
+    dh_stats = None
+    if head == "mixed":
+        ht, hk, hmu, hom = ephmc.convert_params(TRAJ_BETA, NT, J, LAM, 0.0, OMEGA0)
+        hctx = ephmc.Context(L, L, NT, ht, hk, hmu, hom, device=local)
+        lib.ephmc_ctx_set_stream(hctx.h, stream.cuda_stream)
+        xh0 = torch.randn(dim, dtype=torch.float64, device=dev, generator=gen)
+        hctx.fa_scale_free_bosons(xh0)
+        try:
+            ld_h, _ = hctx.eval(xh0, pd, mode="adjoint")
+            d64, dmx, a64, amx = [], [], [], []
+            for _ in range(DH_TRAJ):
+                p0 = torch.randn(dim, dtype=torch.float64, device=dev, generator=gen)
+                hctx.fa_scale_momenta(p0)
+                h0 = hctx.hamilton(xh0, ld_h, hctx.fa_energy(p0))
+                u = urng.random()
+                ends = {}
+                for mode, dl, al in (("adjoint", d64, a64), ("mixed", dmx, amx)):
+                    x1, p1 = xh0.clone(), p0.clone()
+                    hctx.leapfrog(x1, p1, 20, float(np.pi / 2), mode)
+                    ld1, _ = hctx.eval(x1, pd, mode="adjoint")
+                    dl.append(hctx.hamilton(x1, ld1, hctx.fa_energy(p1)) - h0)
+                    al.append(bool(u < np.exp(-dl[-1])))
+                    ends[mode] = (x1, ld1)
+                if a64[-1]:
+                    xh0, ld_h = ends["adjoint"]
+            diff = np.array(dmx) - np.array(d64)
+            dh_stats = {"trajectories": DH_TRAJ, "beta": TRAJ_BETA, "mu0": 0.0,
+                        "mean_abs_dH_fp64": float(np.mean(np.abs(d64))), "mean_dH_fp64": float(np.mean(d64)),
+                        "mean_dH_mixed": float(np.mean(dmx)), "bias": float(np.mean(diff)),
+                        "median_difference": float(np.median(diff)), "max_abs_difference": float(np.max(np.abs(diff))),
+                        "acceptance_fp64": float(np.mean(a64)), "acceptance_mixed": float(np.mean(amx)),
+                        "same_decisions": int(np.sum(np.array(a64) == np.array(amx)))}
+        except ephmc.EphmcError as e:
+            dh_stats = {"failed": str(e)}
+        hctx.close()
+
+    # the 64-chain batch (ephmc_batch_eval), untuned, a few steps
+    batch = None
+    if not args.no_batch:
+        bres = batch_measure(lib, dev, local, batch_chains(), 2, 5, dist, tune=False)
+        nb = len(bres["ctxs"])
+        batch = {"metric": BATCH_METRIC, "value": ws * 5 * nb / bres["batch_s"], "unit": BATCH_UNIT,
+                 "ms_per_step": bres["batch_s"] / 5 * 1e3,
+                 "one_chain_at_a_time": ws * 5 * nb / bres["seq_s"], "e2e": bres["e2e"],
+                 "gpu_launches": bres["launches"], "steps": 5, "warmup": 2,
+                 "workload": f"{nb} chains, L in {{8,12,16,24,32}}, Nt in {{16,32,64}}, beta ~ U[5,40], lambda x "
+                             f"U[0.5,1.5] (seed {BATCH_SEED}), one mixed evaluation per chain per step, not autotuned"}
+        for c in bres["ctxs"]:
+            c.close()
 
     line = None
     if rank == 0:
@@ -723,11 +873,17 @@ def main():
             return ach, (ach / peak if (ach and peak) else None)
 
         kernels = {}
-        for name, flop, ms, pk, bound in (
-                ("k_gj_dataflow (LU, inverse, log det)", LU_FLOP, ph["lu_ms"], fp64, "fp64"),
-                ("k_adjoint_strip (force sweep)" if head == "mixed" else "k_adjoint (force sweep)",
-                 ADJ_SWEEP_FLOP, ph["force_ms"], sweep_peak, "fp32" if head == "mixed" else "fp64"),
-                ("k_slices_strip (M_hat + q stack)", SWEEP1_FLOP, ph["mhat_ms"], fp64, "fp64")):
+        if head == "mixed":
+            phases = (("k_gj_dataflow (LU, inverse, log det)", LU_FLOP, ph["lu_ms"], fp64, "fp64"),
+                      ("force phase: FP64 y chain (k_slices_strip), segment DGEMMs, k_adjoint_strip FP32 sweep",
+                       MIXED_FORCE_FLOP, ph["force_ms"], fp32, "fp32 sweep + fp64 chain/GEMMs"),
+                      ("M_hat phase: k_slices_strip FP64 sweep 1 + segment stacks from the identity",
+                       MIXED_MHAT_FLOP, ph["mhat_ms"], fp64, "fp64"))
+        else:
+            phases = (("k_gj_dataflow (LU, inverse, log det)", LU_FLOP, ph["lu_ms"], fp64, "fp64"),
+                      ("k_adjoint (force sweep)", ADJ_SWEEP_FLOP, ph["force_ms"], sweep_peak, "fp64"),
+                      ("k_slices_strip (M_hat + q stack)", SWEEP1_FLOP, ph["mhat_ms"], fp64, "fp64"))
+        for name, flop, ms, pk, bound in phases:
             ach, fr = frac(flop, ms, pk)
             kernels[name] = {"ms": ms, "achieved_tflops": ach, "peak_tflops": pk, "frac": fr, "bound": bound,
                              "algorithmic_flop_per_launch": flop}
@@ -759,10 +915,13 @@ def main():
                 if ("mixed" in results and "reference" in results) else None,
                 "trajectory": {"ms": traj, "trajectories_per_s": (ws * 1e3 / traj) if traj else None,
                                "beta": TRAJ_BETA, "failed": traj_fail,
-                               "what": "device work of one trajectory at 32x32, Nt=64, beta=10: 20 leapfrog steps "
-                                       "with Fourier acceleration (ephmc_leapfrog, traj_length pi/2) + the "
-                                       "accept-step evaluation; the host momentum draw and the Metropolis scalars "
-                                       "are not included. At beta=20 the MD diverges, in the reference too"},
+                               "acceptance": float(np.mean(traj_acc)) if traj_acc else None,
+                               "what": "wall clock of one whole HMC trajectory at 32x32, Nt=64, beta=10: momentum "
+                                       "draw and Fourier acceleration, action, 20 leapfrog steps with Fourier "
+                                       "acceleration over pi/2 (ephmc_leapfrog), the accept-step evaluation, new "
+                                       "action, Metropolis decision (median of 10 after 2). At beta=20 the MD "
+                                       "diverges, in the reference too"},
+                "mixed_dH": dh_stats, "batch": batch,
                 "roofline": roofline, "fp64_fma_peak_tflops": fp64, "fp32_fma_peak_tflops": fp32,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": results[head]["launches"],
                 "clocks": results[head]["clocks"]}
