@@ -415,11 +415,28 @@ int ensure_seg(ephmc_ctx *c, const SegPlan &p) {
             return ret(EPHMC_ERR_NOMEM, "cuBLAS workspace");
         }
     }
+    if (!c->aux_stream) {
+        if (cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->aux_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->aux_ev[1], cudaEventDisableTiming) != cudaSuccess ||
+            cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess) {
+            cudaGetLastError();
+            return ret(EPHMC_ERR_CUDA, "segmented force: side stream");
+        }
+    }
     cublasHandle_t h = static_cast<cublasHandle_t>(c->blas);
     if (cublasSetStream(h, c->stream) != CUBLAS_STATUS_SUCCESS ||
         cublasSetWorkspace(h, c->blas_ws, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS)
         return ret(EPHMC_ERR_CUDA, "cublasSetStream / cublasSetWorkspace");
     return EPHMC_OK;
+}
+
+// FP32 stacks from the identity (jobs with no source and no destination):
+// the packed FP32 strip kernel where it applies, else the FP64 slice kernel
+// with an FP32 stack
+int launch_identity_stacks(ephmc_ctx *c, const double *x, const SliceJob *jobs_dev, int n) {
+    if (slices_strip_supported(c->lat)) return launch_slices_strip_identity_f32(x, c->c, c->lat, jobs_dev, n, c->stream);
+    return launch_slices<double, double, float>(Axis::Rows, x, c->c, c->lat, jobs_dev, n, c->stream);
 }
 
 // rows of the jobs on the context's lattice: the register-strip kernel where it applies
@@ -428,8 +445,8 @@ int launch_rows(ephmc_ctx *c, const double *x, const SliceJob *jobs_dev, int n) 
     return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, jobs_dev, n, c->stream);
 }
 
-// FP32 stacks from the identity at the top of segment j (j >= 1; segment 0's
-// stack is spilled by sweep 1): q'(t) = B_{t+1}...B_{t1-1} into its region
+// FP32 stack from the identity at the top of segment j:
+// q'(t) = B_{t+1}...B_{t1-1} into its region
 SliceJob seg_identity_job(ephmc_ctx *c, const SegPlan &p, int j) {
     const int t0 = p.b[j + 1], t1 = p.b[j];
     SliceJob jb = job(nullptr, nullptr, t1 - 1, t1 - t0 - 1, -1, 0, kPairs, 1);
@@ -440,9 +457,8 @@ SliceJob seg_identity_job(ephmc_ctx *c, const SegPlan &p, int j) {
 
 // Sweep 1 of the segmented force: M_hat into dst in FP64, the FP64 states at
 // the segment boundaries (one launch per segment, the state passed through
-// memory, the same arithmetic as the whole chain), segment 0's FP32 stack
-// spilled on the way, and (regions) the other segments' FP32 stacks from the
-// identity in one more launch.
+// memory, the same arithmetic as the whole chain), and (regions) every
+// segment's FP32 stack from the identity in one more launch.
 int sweep1_seg(ephmc_ctx *c, const double *x, double *dst) {
     const SegPlan p = seg_plan(c);
     int rc;
@@ -452,21 +468,37 @@ int sweep1_seg(ephmc_ctx *c, const double *x, double *dst) {
         SliceJob jb = job(j == 0 ? nullptr : seg_ck(c, p, j), j == p.m - 1 ? dst : seg_ck(c, p, j + 1), p.b[j] - 1,
                           p.b[j] - p.b[j + 1], -1, 0, kPairs, 1);
         jb.add_identity = (j == p.m - 1) && !(c->flags.zero_filling || c->flags.single_particle);
-        if (j == 0 && p.regions) {
-            jb.stack = seg_region(c, p, 0);
-            jb.stack_off = -1 - p.b[1];
-        }
         v.push_back(jb);
     }
     if ((rc = upload_jobs(c, v, c->jobs))) return rc;
     for (int j = 0; j < p.m && rc == EPHMC_OK; ++j) rc = launch_sweep1(c, x, c->jobs + j, j == 0);
     if (rc || !p.regions) return rc;
+    // every segment's stack from the identity in FP32 (segment 0 too, so that
+    // the whole-stack and the checkpointed forces run the same arithmetic)
     std::vector<SliceJob> id;
-    for (int j = 1; j < p.m; ++j)
+    for (int j = 0; j < p.m; ++j)
         if (p.b[j] - p.b[j + 1] > 1) id.push_back(seg_identity_job(c, p, j));
     if (id.empty()) return EPHMC_OK;
     if ((rc = upload_jobs(c, id, c->jobs + p.m))) return rc;
-    return launch_sweep1(c, x, c->jobs + p.m, true, (int)id.size());
+    // Beside the LU: the dataflow LU (V <= 1024) holds one SM per 8 columns
+    // and leaves the others idle; the FP32 stacks need nothing from sweep 1
+    // or the LU, so they run on a side stream, forked here (after sweep 1, so
+    // they do not slow it) with a grid that fits the idle SMs, and joined
+    // before the force sweep reads them.
+    const int lu_sms = c->V <= 1024 ? (int)((c->V + kLuPanel - 1) / kLuPanel) : c->sm_count;
+    const int free_sms = c->sm_count - lu_sms;
+    if (!slices_strip_supported(c->lat) || free_sms < 8)
+        return launch_identity_stacks(c, x, c->jobs + p.m, (int)id.size());
+    EPHMC_CUDA(cudaEventRecord(c->aux_ev[0], c->stream));
+    EPHMC_CUDA(cudaStreamWaitEvent(c->aux_stream, c->aux_ev[0], 0));
+    // one CTA per SM (launch bound 512 threads, one block per SM) on at most
+    // the idle SMs: the LU's cooperative grid always finds its SMs free
+    if ((rc = launch_slices_strip_identity_f32(x, c->c, c->lat, c->jobs + p.m, (int)id.size(), c->aux_stream,
+                                               free_sms)))
+        return rc;
+    EPHMC_CUDA(cudaEventRecord(c->aux_ev[1], c->aux_stream));
+    c->aux_pending = true;
+    return EPHMC_OK;
 }
 
 // y'(t0) of n segments: yst = ck^T ys (row-major V x V), the n operands and
@@ -520,6 +552,10 @@ int force_mixed_seg(ephmc_ctx *c, const double *x, const double *y0, double logd
         for (int k = 0; k < p.m - 1 && rc == EPHMC_OK; ++k) rc = launch_rows(c, x, c->jobs + 2 * p.m + k, 1);
         if (rc) return rc;
         if (p.m > 1 && (rc = seg_gemm(c, seg_ys(c, p, 1), seg_ck(c, p, 1), seg_yst(c, p, 1), p.m - 1))) return rc;
+        if (c->aux_pending) {  // the stacks from the side stream
+            EPHMC_CUDA(cudaStreamWaitEvent(c->stream, c->aux_ev[1], 0));
+            c->aux_pending = false;
+        }
         rg.seg_j0 = 0;
         rg.y_start = seg_yst(c, p, 0);
         return adjoint(p.m);
@@ -538,7 +574,7 @@ int force_mixed_seg(ephmc_ctx *c, const double *x, const double *y0, double logd
     for (int j = p.m - 1; j >= 0 && rc == EPHMC_OK; --j) {
         if (j < p.m - 1 && (rc = launch_rows(c, x, y_jobs + (p.m - 2 - j), 1))) break;
         if (j > 0 && (rc = seg_gemm(c, Y, seg_ck(c, p, j), yst, 1))) break;
-        if (p.b[j] - p.b[j + 1] > 1 && (rc = launch_sweep1(c, x, id_jobs + j, true))) break;
+        if (p.b[j] - p.b[j + 1] > 1 && (rc = launch_identity_stacks(c, x, id_jobs + j, 1))) break;
         rg.seg_j0 = j;
         rg.zero_force = j == p.m - 1;
         rg.y_start = j > 0 ? yst : Y;
@@ -606,18 +642,21 @@ int stab_issue(ephmc_ctx *c, const double *x, int mode, bool want_force) {
         return launch_adjoint_sweep<float, float>(x, c->c, c->lat, static_cast<const float *>(stack), none, (int)c->nt,
                                                   c->flavors, 0, 0.0, c->force, c->stream, &rg, count);
     };
+    auto launch_stacks = [&](const SliceJob *jd, int n) {
+        return mixed ? launch_identity_stacks(c, x, jd, n) : launch_sweep1(c, x, jd, false, n);
+    };
     auto stacks = [&](int j0, int n) {
         // segments of a single slice have no stack entries
         int rc2 = EPHMC_OK;
         for (int j = j0; j < j0 + n && rc2 == EPHMC_OK; ++j)
-            if (p.b[j] - p.b[j + 1] > 1) rc2 = launch_sweep1(c, x, c->jobs + 2 * p.m + j, mixed);
+            if (p.b[j] - p.b[j + 1] > 1) rc2 = launch_stacks(c->jobs + 2 * p.m + j, 1);
         return rc2;
     };
     if (p.regions) {
         // all segments' stacks in one launch when every segment has entries
         bool all = true;
         for (int j = 0; j < p.m; ++j) all = all && p.b[j] - p.b[j + 1] > 1;
-        rc = all ? launch_sweep1(c, x, c->jobs + 2 * p.m, mixed, p.m) : stacks(0, p.m);
+        rc = all ? launch_stacks(c->jobs + 2 * p.m, p.m) : stacks(0, p.m);
         rg.seg_j0 = 0;
         if (rc == EPHMC_OK) rc = adjoint(p.m);
     }
@@ -1000,6 +1039,9 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     schur_free(c->schur);
     if (c->seg) cudaFree(c->seg);
     stab_free(c->stab);
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+    for (cudaEvent_t e : c->aux_ev)
+        if (e) cudaEventDestroy(e);
     if (c->blas) cublasDestroy(static_cast<cublasHandle_t>(c->blas));
     if (c->blas_ws) cudaFree(c->blas_ws);
     if (c->batch_stream) cudaStreamDestroy(c->batch_stream);

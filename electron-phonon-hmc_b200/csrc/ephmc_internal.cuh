@@ -177,6 +177,12 @@ bool slices_strip_supported(const LatticeDev &lat);
 template <typename StackT>
 int launch_slices_strip(const double *x, const Couplings &c, const LatticeDev &lat, const SliceJob *jobs_dev,
                         int njobs, cudaStream_t st);
+// FP32 (packed pairs) for jobs that start from the identity and spill every
+// state, the last included, to an FP32 stack (dst null): the segmented mixed
+// force's stacks (slices_strip.cu).  max_ctas > 0 caps the grid (the work is
+// taken grid-stride), so that the launch can run on the SMs the LU leaves free.
+int launch_slices_strip_identity_f32(const double *x, const Couplings &c, const LatticeDev &lat,
+                                     const SliceJob *jobs_dev, int njobs, cudaStream_t st, int max_ctas = 0);
 
 // Reference-algorithm refinement + link contraction for slices t0..t0+nb-1:
 //   A_t = pair 1 on columns of G_t, B_t = pair 0 on rows of G_t (already formed),
@@ -352,6 +358,12 @@ struct ephmc_ctx {
     size_t seg_bytes = 0;
     void *blas = nullptr;       // cublasHandle_t
     void *blas_ws = nullptr;
+    // the segment stacks run on a side stream beside the LU, on the SMs it
+    // leaves idle: fork after sweep 1, join before the force sweep
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t aux_ev[2] = {nullptr, nullptr};
+    bool aux_pending = false;
+    int sm_count = 0;
     // ephmc_batch_eval: the context's own non-blocking stream, used in place of
     // the legacy default stream so that chains overlap; created on first use
     cudaStream_t batch_stream = nullptr;

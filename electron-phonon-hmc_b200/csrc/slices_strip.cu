@@ -17,6 +17,8 @@
 // eight operand loads/stores to the strip ends' share.
 #include "ephmc_internal.cuh"
 
+#include <algorithm>
+
 namespace ephmc {
 
 namespace {
@@ -201,5 +203,169 @@ template int launch_slices_strip<float>(const double *, const Couplings &, const
                                         cudaStream_t);
 template int launch_slices_strip<double>(const double *, const Couplings &, const LatticeDev &, const SliceJob *,
                                          int, cudaStream_t);
+
+}  // namespace ephmc
+
+// ---------------------------------------------------------------- FP32 variant
+// The stacks of the segmented mixed force start from the identity at each
+// segment's top and run at most one segment (<= 16 slices by default), so they
+// are propagated in FP32: the two vectors of a CTA are the halves of float2
+// pairs and every stencil is one packed FP32 instruction (fma/mul/add
+// .rn.f32x2) for both.  Same layout as the FP64 kernel above.
+namespace ephmc {
+
+namespace {
+
+using P2 = float2;
+__device__ __forceinline__ P2 p2fma(P2 a, P2 b, P2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ P2 p2mul(P2 a, P2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ P2 p2add(P2 a, P2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ P2 p2dup(float c) { return make_float2(c, c); }
+__device__ __forceinline__ P2 p2shfl(P2 v, int src) {
+    return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+struct HopF {
+    P2 f0, f1, f2, f0l, f1d, f2dr;
+};
+
+__device__ __forceinline__ P2 stencil_f(const HopF &h, P2 mu, P2 v, P2 l, P2 r, P2 up, P2 down, P2 upleft,
+                                        P2 downright) {
+    const P2 s1 = p2fma(h.f0, r, p2mul(mu, v));
+    const P2 s2 = p2fma(h.f1, up, p2mul(h.f0l, l));
+    const P2 s3 = p2fma(h.f2, upleft, p2mul(h.f1d, down));
+    return p2add(p2add(s1, s2), p2fma(h.f2dr, downright, s3));
+}
+
+__device__ __forceinline__ void group_bar(int g, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(nthreads) : "memory");
+}
+
+// w = (mu + K) v for the thread's H sites of both vectors; edge rows through
+// shared memory (edge[2][nw][32] pairs of the thread's group), one group
+// barrier before and one after
+template <int H>
+__device__ __forceinline__ void apply_H_f(const P2 (&v)[H], P2 (&w)[H], const HopF (&hp)[H], P2 mu, P2 *edge, int nw,
+                                          int warp, int lane, int g) {
+    const int below = (warp + nw - 1) % nw, above = (warp + 1) % nw;
+    P2 *bot = edge, *top = edge + (size_t)nw * 32;
+    bot[warp * 32 + lane] = v[0];
+    top[warp * 32 + lane] = v[H - 1];
+    group_bar(g, 32 * nw);
+    const int lm = (lane + 31) & 31, lp = (lane + 1) & 31;
+    const P2 dn = top[below * 32 + lane];
+    const P2 upx = bot[above * 32 + lane];
+    P2 L[H], Rt[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+        L[h] = p2shfl(v[h], lm);
+        Rt[h] = p2shfl(v[h], lp);
+    }
+    const P2 dnR = p2shfl(dn, lp), upL = p2shfl(upx, lm);
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+        const P2 up = (h + 1 < H) ? v[h + 1] : upx;
+        const P2 down = (h > 0) ? v[h - 1] : dn;
+        const P2 ul = (h + 1 < H) ? L[h + 1] : upL;
+        const P2 dr = (h > 0) ? Rt[h - 1] : dnR;
+        w[h] = stencil_f(hp[h], mu, v[h], L[h], Rt[h], up, down, ul, dr);
+    }
+    group_bar(g, 32 * nw);
+}
+
+// jobs with an identity start and no destination (every state, the last
+// included, goes to the FP32 stack).  A CTA has G independent groups of
+// nw = L2/H warps (named barriers per group); work item = (job, vector pair),
+// taken grid-stride by the groups, so that a grid of one CTA per SM can run
+// beside the LU on the SMs the LU leaves idle.
+template <int H, int G>
+__global__ void __launch_bounds__(512, 1) k_slices_strip_f32(const double *__restrict__ x, Couplings cp,
+                                                             const SliceJob *__restrict__ jobs, int njobs, int L2) {
+    extern __shared__ P2 edge_f[];  // [G][2][nw][32]
+    const int lane = threadIdx.x & 31, nw = L2 / H;
+    const int g = (int)(threadIdx.x >> 5) / nw, warp = (int)(threadIdx.x >> 5) - g * nw;
+    P2 *edge_g = edge_f + (size_t)g * 2 * nw * 32;
+    const int V = 32 * L2;
+    const size_t VV = (size_t)V * V;
+    const int b0 = H * warp;
+    const P2 mu = p2dup((float)cp.mu);
+    const int pairs = V / 2;  // V = 32 L2 is even: both vectors of a pair live
+    for (int item = blockIdx.x * G + g; item < njobs * pairs; item += gridDim.x * G) {
+    const SliceJob job = jobs[item / pairs];
+    const int c0 = (item % pairs) * 2, c1 = c0 + 1;
+    P2 v[H], w[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+        const int i = (b0 + h) * 32 + lane;
+        v[h] = make_float2(i == c0 ? 1.f : 0.f, i == c1 ? 1.f : 0.f);
+    }
+    const int lm = (lane + 31) & 31, lp = (lane + 1) & 31;
+    for (int it = 0; it < job.s_count; ++it) {
+        const int sl = job.s_first + it * job.s_dir;
+        const double *xs = x + (size_t)sl * 3 * V;
+        HopF hp[H];
+        {
+            const int bd = (b0 + L2 - 1) % L2;
+            float f1p = (float)fma(-cp.kappa[1], xs[3 * (bd * 32 + lane) + 1], cp.t[1]);
+            float f2p = (float)fma(-cp.kappa[2], xs[3 * (bd * 32 + lane) + 2], cp.t[2]);
+#pragma unroll
+            for (int h = 0; h < H; ++h) {
+                const int i = (b0 + h) * 32 + lane;
+                const float f0 = (float)fma(-cp.kappa[0], xs[3 * i + 0], cp.t[0]);
+                const float f1 = (float)fma(-cp.kappa[1], xs[3 * i + 1], cp.t[1]);
+                const float f2 = (float)fma(-cp.kappa[2], xs[3 * i + 2], cp.t[2]);
+                hp[h].f0 = p2dup(f0);
+                hp[h].f1 = p2dup(f1);
+                hp[h].f2 = p2dup(f2);
+                hp[h].f0l = p2dup(__shfl_sync(0xffffffffu, f0, lm));
+                hp[h].f1d = p2dup(f1p);
+                hp[h].f2dr = p2dup(__shfl_sync(0xffffffffu, f2p, lp));
+                f1p = f1;
+                f2p = f2;
+            }
+        }
+        for (int p = job.p_begin; p != job.p_end; p += job.p_step) {
+            const P2 al = p2dup((float)(p ? cp.a_lin[1] : cp.a_lin[0]));
+            const P2 aq = p2dup((float)(p ? cp.a_quad[1] : cp.a_quad[0]));
+            apply_H_f<H>(v, w, hp, mu, edge_g, nw, warp, lane, g);
+            if (p ? cp.cplx[1] : cp.cplx[0]) {
+                P2 z[H];
+                apply_H_f<H>(w, z, hp, mu, edge_g, nw, warp, lane, g);
+#pragma unroll
+                for (int h = 0; h < H; ++h) v[h] = p2add(v[h], p2fma(al, w[h], p2mul(aq, z[h])));
+            } else {
+#pragma unroll
+                for (int h = 0; h < H; ++h) v[h] = p2fma(al, w[h], v[h]);
+            }
+        }
+        float *dst = static_cast<float *>(job.stack) + (size_t)(sl + job.stack_off) * VV;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const int i = (b0 + h) * 32 + lane;
+            dst[(size_t)c0 * V + i] = v[h].x;
+            dst[(size_t)c1 * V + i] = v[h].y;
+        }
+    }
+    }
+}
+
+}  // namespace
+
+int launch_slices_strip_identity_f32(const double *x, const Couplings &c, const LatticeDev &lat,
+                                     const SliceJob *jobs_dev, int njobs, cudaStream_t st, int max_ctas) {
+    if (!slices_strip_supported(lat)) return EPHMC_ERR_UNSUPPORTED;
+    if (njobs <= 0) return EPHMC_OK;
+    constexpr int H = 4, G = 2;
+    const int V = lat.V, L2 = lat.l2, nw = L2 / H;
+    if (G * nw * 32 > 512) return EPHMC_ERR_UNSUPPORTED;
+    const size_t smem = sizeof(P2) * G * 2 * (size_t)nw * 32;
+    const int items = njobs * (V / 2);
+    const int need = (items + G - 1) / G;
+    const int grid = max_ctas > 0 ? std::min(need, max_ctas) : need;
+    k_slices_strip_f32<H, G><<<grid, G * 32 * nw, smem, st>>>(x, c, jobs_dev, njobs, L2);
+    count_launch(1);
+    EPHMC_CUDA(cudaGetLastError());
+    return EPHMC_OK;
+}
 
 }  // namespace ephmc
