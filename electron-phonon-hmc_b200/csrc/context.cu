@@ -1039,6 +1039,7 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     schur_free(c->schur);
     if (c->seg) cudaFree(c->seg);
     stab_free(c->stab);
+    cudaFree(c->dropin_block);
     if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     for (cudaEvent_t e : c->aux_ev)
         if (e) cudaEventDestroy(e);

@@ -353,6 +353,8 @@ struct ephmc_ctx {
     // first use; the cuBLAS handle of its Z GEMMs and that handle's workspace
     unsigned seg_len = 0;       // ephmc_ctx_set_segment (0: the built-in rule)
     bool stabilize = false;     // ephmc_ctx_set_stabilize: UDT-stabilised chain (stabilize.cu)
+    double *dropin_block = nullptr;  // the drop-in trajectory's device state block (host callers)
+    size_t dropin_block_n = 0;
     ephmc::StabWork *stab = nullptr;
     double *seg = nullptr;
     size_t seg_bytes = 0;

@@ -470,6 +470,13 @@ void leap_frog(double *x, double *p, double *p_dot, ephmc_dcomplex *xc, double *
 }
 
 // trajectory (simulation/organic_hmc.c:192-294): x is the base of the reference's block
+// x | p | p_dot | x_old | M_hat | M_hat_old | QM1P[Nt V^2] | R_0t | w[5 V^2].
+// A device block is used in place.  For a host block the context keeps a
+// device block of that layout between calls, and a call moves only what the
+// trajectory reads (x and M_hat, the current field and its inverse) and the
+// parts a caller can use afterwards (x, p, p_dot, x_old, M_hat, M_hat_old);
+// the rest is work space (QM1P, R_0t, w), about (Nt + 6) V^2 doubles that are
+// not copied.
 short trajectory(double *x, ephmc_dcomplex *xc, int *perm, double *t, double *kappa, double mu, double omega,
                  unsigned flavors, double *contr_mat, unsigned *nnt, unsigned ns, unsigned, unsigned nt, unsigned steps,
                  double traj_length, double *results, double *greens, int iteration, unsigned meas_freq,
@@ -480,10 +487,29 @@ short trajectory(double *x, ephmc_dcomplex *xc, int *perm, double *t, double *ka
     ephmc_ctx *c = ctx_for(nnt, ns, nt, t, kappa, mu, omega, flavors, mode);
     if (!c) return 0;
     const size_t dim = (size_t)nt * ns * 3, VV = (size_t)ns * ns;
-    Dev B(x, 4 * dim + (8 + (size_t)nt) * VV);
-    const short acc = trajectory_dev(c, B.d, results, greens, iteration, meas_freq, contr_mat, steps, traj_length,
-                                     old, res_out, corr_out);
-    B.back();
+    const size_t total = 4 * dim + (8 + (size_t)nt) * VV;
+    if (devp(x))
+        return trajectory_dev(c, x, results, greens, iteration, meas_freq, contr_mat, steps, traj_length, old, res_out,
+                              corr_out);
+    if (c->dropin_block_n < total) {
+        cudaFree(c->dropin_block);
+        c->dropin_block = nullptr;
+        c->dropin_block_n = 0;
+        if (cudaMalloc(&c->dropin_block, sizeof(double) * total) != cudaSuccess) {
+            cudaGetLastError();
+            std::fprintf(stderr, "ephmc trajectory: no device memory for the state block\n");
+            return 0;
+        }
+        c->dropin_block_n = total;
+    }
+    double *d = c->dropin_block;
+    const size_t off_M = 4 * dim;
+    cudaMemcpy(d, x, sizeof(double) * dim, cudaMemcpyHostToDevice);                      // x
+    cudaMemcpy(d + off_M, x + off_M, sizeof(double) * VV, cudaMemcpyHostToDevice);      // M_hat
+    const short acc = trajectory_dev(c, d, results, greens, iteration, meas_freq, contr_mat, steps, traj_length, old,
+                                     res_out, corr_out);
+    cudaMemcpy(x, d, sizeof(double) * 4 * dim, cudaMemcpyDeviceToHost);                 // x, p, p_dot, x_old
+    cudaMemcpy(x + off_M, d + off_M, sizeof(double) * 2 * VV, cudaMemcpyDeviceToHost);  // M_hat, M_hat_old
     return acc;
 }
 

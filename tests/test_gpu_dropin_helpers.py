@@ -183,3 +183,54 @@ def test_cc_correlator_at_32x32(gpu, reference, restated):
     print(f"cc_correlator 32x32 Nt=64: {err:.2e} of the largest entry; {1e3 * dt:.1f} ms per call with host "
           f"buffers (R_t0 back to the host: {Rt0.nbytes / 1e6:.0f} MB)")
     assert err <= 1e-10
+
+
+def test_trajectory_host_block_equals_device_block(gpu, restated):
+    """trajectory() (simulation/organic_hmc.c:192-294) with the reference's
+    state block in host memory (the library keeps a device block and moves
+    only x, M_hat in and x, p, p_dot, x_old, M_hat, M_hat_old out) against
+    the same call with the block in device memory, on the same random
+    stream: same Metropolis decision, field, inverse and log det."""
+    import torch
+
+    import ephmc
+    from oracle import Model
+    lib = ephmc.load_library()
+    lib.ephmc_rng_seed.argtypes = [C.c_ulonglong]
+    lib.ephmc_rng_seed.restype = None
+    lib.construct_M_hat.argtypes = [P, P, P, P, P, D, P, U, U, U, P]
+    lib.construct_M_hat.restype = None
+    lib.logDetM_and_inv_M_hat.argtypes = [P, P, P, U, U, P]
+    lib.logDetM_and_inv_M_hat.restype = D
+    lib.trajectory.argtypes = [P, P, P, P, P, D, D, U, P, P, U, U, U, U, D, P, P, I, U, P, P, P, P, P]
+    lib.trajectory.restype = C.c_short
+    m = Model.physical(6, 6, 16, 4.0, mu0=1.0)
+    nnt = restated.lattice(m.l1, m.l2)
+    t, kap = np.array(m.t), np.array(m.kappa)
+    dim, VV = m.dim, m.ns * m.ns
+    flags = OrganicFlags()
+    block0 = np.zeros(4 * dim + (8 + m.nt) * VV)
+    block0[:dim] = 0.3 * restated.random_x(21, dim)
+    w = np.empty(5 * VV)
+    perm = np.zeros(max(m.ns, 2 * m.nt), dtype=np.int32)
+    M = block0[4 * dim: 4 * dim + VV]
+    lib.construct_M_hat(_p(block0), _p(M), _p(w), _p(t), _p(kap), m.mu, _p(nnt), m.ns, 6, m.nt, C.byref(flags))
+    ld0 = lib.logDetM_and_inv_M_hat(_p(M), _p(w), _p(perm), m.ns, 1, C.byref(flags))
+    out = []
+    for on_device in (False, True):
+        for seed in (31, 32):
+            lib.ephmc_rng_seed(seed)
+            old = np.array([ld0])
+            blk = block0.copy()
+            bd = torch.from_numpy(blk).cuda() if on_device else None
+            acc = lib.trajectory(bd.data_ptr() if on_device else _p(blk), None, None, _p(t), _p(kap), m.mu, m.omega,
+                                 1, None, _p(nnt), m.ns, 6, m.nt, 3, np.pi / 2, None, None, 1, 1, None, _p(old), None, None,
+                                 C.byref(flags))
+            if on_device:
+                blk = bd.cpu().numpy()
+            out.append((acc, blk[:dim].copy(), blk[4 * dim: 4 * dim + VV].copy(), old[0]))
+    for (a0, x0, m0, l0), (a1, x1, m1, l1) in zip(out[:2], out[2:]):
+        assert a0 == a1
+        assert np.max(np.abs(x0 - x1)) <= 1e-12 * np.max(np.abs(x1))
+        assert np.max(np.abs(m0 - m1)) <= 1e-12 * np.max(np.abs(m1))
+        assert abs(l0 - l1) <= 1e-12 * abs(l1)
