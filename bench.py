@@ -18,6 +18,9 @@ replicas (one process per GPU, no data-path collective).
 and coupling evaluated together (ephmc_batch_eval), against the same chains
 one at a time.
 
+`--workload stabilised` times the mixed force on the re-stabilised FP64 chain
+(ephmc_ctx_set_stabilize) at 48x48, Nt = 128, beta = 40.
+
 `--workload trans_loc` measures the static-disorder mode instead:
 disorder samples/s of hist_trans_loc (simulation/organic_trans_loc.c:25-83) on
 a 64x64 lattice (V = 4096) with 512 frequency bins, beta = 40, one step = one
@@ -77,6 +80,57 @@ TL_A, TL_B = (1.0, 0.0), (0.5, 0.8660254)
 TL_METRIC = "disorder samples/s, TL mode 64x64 lattice (V=4096), 512 bins, beta=40"
 TL_UNIT = "samples/s"
 TL_WORKLOAD = "static disorder: 64x64 triangular lattice (V=4096), 512 frequency bins, beta=40, mu0=0"
+
+
+# the checkpointing configuration at its own temperature, where the raw slice
+# product loses log det to rounding: the re-stabilised chain (48x48, Nt = 128,
+# beta = 40, checkpoints every 12 slices, stabilisation segments of 6)
+STAB_L, STAB_NT, STAB_BETA, STAB_CKPT = 48, 128, 40.0, 12
+STAB_METRIC = "stabilised force+logdet evals/s, 48x48 lattice Nt=128 beta=40 (re-stabilised FP64 chain)"
+
+
+def run_stabilised_bench(args):
+    """evals/s of the mixed force on the re-stabilised chain (ephmc_ctx_set_stabilize):
+    W warm-up and K timed evaluations on device-resident N(0,1) fields, beside
+    the unstabilised evaluation of the same context for comparison."""
+    import torch
+
+    import ephmc
+    ws, rank, local = dist_env()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = ephmc.load_library()
+    L_, nt = args.stab_l, STAB_NT
+    t, kappa, mu, omega = ephmc.convert_params(STAB_BETA, nt, J, LAM, MU0, OMEGA0)
+    ctx = ephmc.Context(L_, L_, nt, t, kappa, mu, omega, device=local)
+    ctx.set_checkpoint(STAB_CKPT)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(99 + rank)
+    x = torch.randn(ctx.dim, dtype=torch.float64, device=dev, generator=gen)
+    pd = torch.empty_like(x)
+    W, K = max(1, min(args.warmup, 3)), max(1, min(args.steps, 10))
+    out = {}
+    for stab in ((True,) if args.profile else (False, True)):
+        ctx.set_stabilize(stab)
+        for _ in range(W):
+            ctx.eval(x, pd, mode="mixed")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            ctx.eval(x, pd, mode="mixed")
+        torch.cuda.synchronize()
+        out[stab] = (time.perf_counter() - t0) / K
+    ctx.close()
+    if args.profile or rank != 0:
+        return 0
+    print(json.dumps({"metric": STAB_METRIC, "value": 1.0 / out[True], "unit": UNIT, "n_gpus": 1, "steps": K,
+                      "warmup": W, "ms_per_step": 1e3 * out[True], "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+                      "config": {"workload": f"{L_}x{L_} lattice, Nt={nt}, beta={STAB_BETA}, checkpoints every "
+                                             f"{STAB_CKPT} slices, stabilisation segments of 6, mixed force",
+                                 "inputs": "x ~ N(0,1) (torch.randn)"},
+                      "unstabilised_ms_per_eval": 1e3 * out[False]}), flush=True)
+    return 0
 
 
 def tl_params():
@@ -651,11 +705,14 @@ def main():
     ap.add_argument("--paths", default="mixed,adjoint,reference")
     ap.add_argument("--profile", action="store_true",
                     help="run only warm-up + timed evaluations of --paths (for ncu); print nothing")
-    ap.add_argument("--workload", default="hmc", choices=["hmc", "trans_loc", "batch"])
+    ap.add_argument("--workload", default="hmc", choices=["hmc", "trans_loc", "batch", "stabilised"])
+    ap.add_argument("--stab-l", type=int, default=STAB_L, help="stabilised: lattice extent")
     ap.add_argument("--tl-batch", type=int, default=16, help="trans_loc: disorder samples per step")
     ap.add_argument("--tl-lanes", type=int, default=2, help="trans_loc: samples diagonalised concurrently")
     ap.add_argument("--tl-l", type=int, default=TL_L, help="trans_loc: lattice extent (profiling on smaller cases)")
     args = ap.parse_args()
+    if args.workload == "stabilised":
+        return 0 if args.impl == "reference" else run_stabilised_bench(args)
     if args.workload == "trans_loc":
         return run_reference_trans_loc(args) if args.impl == "reference" else run_trans_loc_bench(args)
     if args.workload == "batch":

@@ -47,15 +47,31 @@
 
 namespace ephmc {
 
-struct StabWork {
-    int V = 0, m = 0;
+// The Q side and the P side of the chain are independent until the segment
+// factors: the P side runs on a second stream (lane 1) with its own handles
+// and temporaries.
+struct StabLane {
+    cudaStream_t st = nullptr;
     cusolverDnHandle_t sol = nullptr;
     cublasHandle_t blas = nullptr;
-    double *ws = nullptr;  // cuSOLVER workspace
+    double *ws = nullptr;    // cuSOLVER workspace (lwork doubles)
+    int *info = nullptr;     // device: [0] solver info, [1] sign accumulator (+-1)
+    double *tau = nullptr, *norms = nullptr;  // V each
+    int *perm = nullptr;     // V
+};
+
+struct StabWork {
+    int V = 0, m = 0;
+    StabLane lane[2];        // lane 0 on the context's stream, lane 1 on its own
+    cudaEvent_t ev[2] = {nullptr, nullptr};  // fork to and join from lane 1
+    double *lane_buf = nullptr;  // lanes' workspaces, infos and vectors
     int lwork = 0;
-    int *info = nullptr;   // device: [0] solver info, [1] sign accumulator (+-1) of det T_0
-    double *mats = nullptr;  // (6m + 2) V^2: U, Ti, SU, Up, Tpi, yst (m each), N, W
-    double *vecs = nullptr;  // 2 m V (d, d') + 3 V (tau, norms, whole-product d) + 8 (log det parts)
+    cusolverDnHandle_t sol = nullptr;  // = lane[0].sol
+    cublasHandle_t blas = nullptr;     // = lane[0].blas
+    double *ws = nullptr;
+    int *info = nullptr;
+    double *mats = nullptr;  // (6m + 3) V^2: U, Ti, SU, Up, Tpi, yst (m each), N, W, and lane 1's W
+    double *vecs = nullptr;  // 2 m V (d, d') + 3 V (tau, norms: unused, whole-product d) + 8 (log det parts)
     int *ivecs = nullptr;    // 2 V: sort permutation, LU pivots
     void *stack = nullptr;   // segment stacks when the context's q stack is too small
     size_t stack_bytes = 0;
@@ -68,6 +84,7 @@ struct StabWork {
     double *yst(int j) const { return mats + (size_t)(5 * m + j) * VV(); }  // top-down segment index
     double *N() const { return mats + (size_t)(6 * m) * VV(); }
     double *W() const { return mats + (size_t)(6 * m + 1) * VV(); }
+    double *W1() const { return mats + (size_t)(6 * m + 2) * VV(); }
     double *d(int k) const { return vecs + (size_t)k * V; }
     double *dp(int k) const { return vecs + (size_t)(m + k) * V; }
     double *tau() const { return vecs + (size_t)2 * m * V; }
@@ -285,26 +302,27 @@ int fail(int st, const char *msg) {
 // One UDT step: (S U) diag(d_in) = U_out diag(d_out) R Pi^T; Ti_out = Ti_in Pi R^-1 diag(d_out).
 // SU: the segment applied to U_in (column-major); acc: det T sign accumulator
 // or null; q_sign: also multiply the accumulator by sign(det U_out).
-int qr_step(StabWork &w, const double *SU, const double *d_in, const double *Ti_in, double *U_out, double *d_out,
-            double *Ti_out, int *acc, cudaStream_t st, bool q_sign = false) {
+int qr_step(StabWork &w, StabLane &ln, const double *SU, const double *d_in, const double *Ti_in, double *U_out,
+            double *d_out, double *Ti_out, int *acc, bool q_sign = false) {
     const int V = w.V;
     const size_t VV = w.VV();
-    k_colnorm<<<blocks((size_t)V * 32), 256, 0, st>>>(SU, d_in, V, w.norms());
-    k_argsort_desc<<<1, 1024, 0, st>>>(w.norms(), V, w.perm());
-    k_gather_cols<<<blocks(VV), 256, 0, st>>>(SU, d_in, w.perm(), V, U_out);
-    k_gather_cols<<<blocks(VV), 256, 0, st>>>(Ti_in, nullptr, w.perm(), V, Ti_out);
+    cudaStream_t st = ln.st;
+    k_colnorm<<<blocks((size_t)V * 32), 256, 0, st>>>(SU, d_in, V, ln.norms);
+    k_argsort_desc<<<1, 1024, 0, st>>>(ln.norms, V, ln.perm);
+    k_gather_cols<<<blocks(VV), 256, 0, st>>>(SU, d_in, ln.perm, V, U_out);
+    k_gather_cols<<<blocks(VV), 256, 0, st>>>(Ti_in, nullptr, ln.perm, V, Ti_out);
     count_launch(4);
-    STAB_SOLVER(cusolverDnDgeqrf(w.sol, V, V, U_out, V, w.tau(), w.ws, w.lwork, w.info));
-    k_qr_diag<<<1, 1024, 0, st>>>(U_out, w.perm(), V, d_out, acc);
+    STAB_SOLVER(cusolverDnDgeqrf(ln.sol, V, V, U_out, V, ln.tau, ln.ws, w.lwork, ln.info));
+    k_qr_diag<<<1, 1024, 0, st>>>(U_out, ln.perm, V, d_out, acc);
     count_launch(1);
     const double one = 1.0;
-    STAB_BLAS(cublasDtrsm(w.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, V, V,
+    STAB_BLAS(cublasDtrsm(ln.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, V, V,
                           &one, U_out, V, Ti_out, V));
     k_scale_cols<<<blocks(VV), 256, 0, st>>>(Ti_out, d_out, V);
     count_launch(1);
-    STAB_SOLVER(cusolverDnDorgqr(w.sol, V, V, V, U_out, V, w.tau(), w.ws, w.lwork, w.info));
+    STAB_SOLVER(cusolverDnDorgqr(ln.sol, V, V, V, U_out, V, ln.tau, ln.ws, w.lwork, ln.info));
     if (acc != nullptr && q_sign) {
-        k_tau_sign<<<1, 1024, 0, st>>>(w.tau(), V, acc);  // det U_out: its Householder reflectors
+        k_tau_sign<<<1, 1024, 0, st>>>(ln.tau, V, acc);  // det U_out: its Householder reflectors
         count_launch(1);
     }
     count_launch(3);
@@ -316,10 +334,14 @@ int qr_step(StabWork &w, const double *SU, const double *d_in, const double *Ti_
 
 void stab_free(StabWork *w) {
     if (!w) return;
-    if (w->sol) cusolverDnDestroy(w->sol);
-    if (w->blas) cublasDestroy(w->blas);
-    cudaFree(w->ws);
-    cudaFree(w->info);
+    for (StabLane &ln : w->lane) {
+        if (ln.sol) cusolverDnDestroy(ln.sol);
+        if (ln.blas) cublasDestroy(ln.blas);
+    }
+    if (w->lane[1].st) cudaStreamDestroy(w->lane[1].st);
+    for (cudaEvent_t e : w->ev)
+        if (e) cudaEventDestroy(e);
+    cudaFree(w->lane_buf);
     cudaFree(w->mats);
     cudaFree(w->vecs);
     cudaFree(w->ivecs);
@@ -329,8 +351,9 @@ void stab_free(StabWork *w) {
 
 size_t stab_bytes(const StabWork *w) {
     if (!w || !w->mats) return 0;
-    return sizeof(double) * ((6 * (size_t)w->m + 2) * w->VV() + (2 * (size_t)w->m + 3) * w->V + 8 + w->lwork) +
-           sizeof(int) * (2 * (size_t)w->V + 2) + w->stack_bytes;
+    return sizeof(double) * ((6 * (size_t)w->m + 3) * w->VV() + (2 * (size_t)w->m + 3) * w->V + 8) +
+           2 * (sizeof(double) * ((size_t)w->lwork + 2 * w->V + 1) + sizeof(int) * (size_t)w->V) +
+           sizeof(int) * 2 * (size_t)w->V + w->stack_bytes;
 }
 
 // Buffers for m segments of a V-site lattice (reallocated when m changes).
@@ -340,16 +363,24 @@ static int stab_ensure(StabWork **slot, int V, int m, cudaStream_t st) {
     if (!w) {
         w = new StabWork();
         *slot = w;
-        if (cusolverDnCreate(&w->sol) != CUSOLVER_STATUS_SUCCESS || cublasCreate(&w->blas) != CUBLAS_STATUS_SUCCESS)
-            return fail(EPHMC_ERR_CUDA, "stabilised chain: cuSOLVER / cuBLAS handle");
+        for (StabLane &ln : w->lane)
+            if (cusolverDnCreate(&ln.sol) != CUSOLVER_STATUS_SUCCESS || cublasCreate(&ln.blas) != CUBLAS_STATUS_SUCCESS)
+                return fail(EPHMC_ERR_CUDA, "stabilised chain: cuSOLVER / cuBLAS handle");
+        if (cudaStreamCreateWithFlags(&w->lane[1].st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&w->ev[0], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&w->ev[1], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(EPHMC_ERR_CUDA, "stabilised chain: second stream");
+        }
+        w->sol = w->lane[0].sol;
+        w->blas = w->lane[0].blas;
     }
     if (w->V != V || w->m != m) {
-        cudaFree(w->ws);
-        cudaFree(w->info);
+        cudaFree(w->lane_buf);
         cudaFree(w->mats);
         cudaFree(w->vecs);
         cudaFree(w->ivecs);
-        w->ws = w->mats = w->vecs = nullptr;
+        w->lane_buf = w->mats = w->vecs = w->ws = nullptr;
         w->info = w->ivecs = nullptr;
         w->V = V;
         w->m = m;
@@ -361,18 +392,33 @@ static int stab_ensure(StabWork **slot, int V, int m, cudaStream_t st) {
             return fail(EPHMC_ERR_CUDA, "stabilised chain: workspace query");
         w->lwork = std::max({l1, l2, l3, 1});
         const size_t VV = (size_t)V * V;
-        if (cudaMalloc((void **)&w->ws, sizeof(double) * w->lwork) != cudaSuccess ||
-            cudaMalloc((void **)&w->info, sizeof(int) * 2) != cudaSuccess ||
-            cudaMalloc((void **)&w->mats, sizeof(double) * (6 * (size_t)m + 2) * VV) != cudaSuccess ||
+        // per lane: workspace, 2 info words (as one double), tau, norms, perm
+        const size_t per_lane = (size_t)w->lwork + 1 + 2 * (size_t)V + ((size_t)V + 1) / 2;
+        if (cudaMalloc((void **)&w->lane_buf, sizeof(double) * 2 * per_lane) != cudaSuccess ||
+            cudaMalloc((void **)&w->mats, sizeof(double) * (6 * (size_t)m + 3) * VV) != cudaSuccess ||
             cudaMalloc((void **)&w->vecs, sizeof(double) * ((2 * (size_t)m + 3) * V + 8)) != cudaSuccess ||
             cudaMalloc((void **)&w->ivecs, sizeof(int) * 2 * (size_t)V) != cudaSuccess) {
             cudaGetLastError();
             w->V = w->m = 0;
             return fail(EPHMC_ERR_NOMEM, "stabilised chain buffers");
         }
+        for (int l = 0; l < 2; ++l) {
+            double *base = w->lane_buf + (size_t)l * per_lane;
+            StabLane &ln = w->lane[l];
+            ln.ws = base;
+            ln.info = reinterpret_cast<int *>(base + w->lwork);
+            ln.tau = base + w->lwork + 1;
+            ln.norms = ln.tau + V;
+            ln.perm = reinterpret_cast<int *>(ln.norms + V);
+        }
+        w->ws = w->lane[0].ws;
+        w->info = w->lane[0].info;
     }
-    if (cusolverDnSetStream(w->sol, st) != CUSOLVER_STATUS_SUCCESS || cublasSetStream(w->blas, st) != CUBLAS_STATUS_SUCCESS)
-        return fail(EPHMC_ERR_CUDA, "stabilised chain: set stream");
+    w->lane[0].st = st;
+    for (StabLane &ln : w->lane)
+        if (cusolverDnSetStream(ln.sol, ln.st) != CUSOLVER_STATUS_SUCCESS ||
+            cublasSetStream(ln.blas, ln.st) != CUBLAS_STATUS_SUCCESS)
+            return fail(EPHMC_ERR_CUDA, "stabilised chain: set stream");
     return EPHMC_OK;
 }
 
@@ -409,7 +455,7 @@ int stab_chain(ephmc_ctx *c, StabWork **slot, const double *x, const std::vector
         for (int k = 0; k + 1 < m; ++k) {
             SliceJob j{};
             j.src = k == 0 ? nullptr : w.Up(k);
-            j.dst = w.W();
+            j.dst = w.W1();
             j.s_first = seg_s(k);
             j.s_count = seg_e(k) - seg_s(k);
             j.s_dir = +1;
@@ -419,80 +465,83 @@ int stab_chain(ephmc_ctx *c, StabWork **slot, const double *x, const std::vector
             jobs.push_back(j);
         }
     if ((rc = ctx_upload_jobs(c, jobs.data(), (int)jobs.size(), slot0, st))) return rc;
-    auto apply = [&](int ji) {
-        if (slices_strip_supported(c->lat)) return launch_slices_strip<double>(x, c->c, c->lat, jobs_dev + ji, 1, st);
-        return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, jobs_dev + ji, 1, st);
+    auto apply = [&](int ji, cudaStream_t s2) {
+        if (slices_strip_supported(c->lat)) return launch_slices_strip<double>(x, c->c, c->lat, jobs_dev + ji, 1, s2);
+        return launch_slices<double, double, double>(Axis::Rows, x, c->c, c->lat, jobs_dev + ji, 1, s2);
     };
-    // Q side, top down: U_{m-1} = 1, d = 1, T^-1 = 1
+    StabLane &q = w.lane[0], &pl = w.lane[1];
+    const double one = 1.0, zero = 0.0;
+    // P side, bottom up, on lane 1 (forked after the job upload): U'_0 = 1,
+    // d' = 1, T'^-1 = 1; each step applies S_k^T to U'_k in lane 1's W
+    if (want_z) {
+        EPHMC_CUDA(cudaEventRecord(w.ev[0], st));
+        EPHMC_CUDA(cudaStreamWaitEvent(pl.st, w.ev[0], 0));
+        k_eye<<<blocks(VV), 256, 0, pl.st>>>(w.Up(0), V);
+        k_eye<<<blocks(VV), 256, 0, pl.st>>>(w.Tpi(0), V);
+        k_ones<<<blocks(V), 256, 0, pl.st>>>(w.dp(0), V, nullptr);
+        count_launch(3);
+        for (int k = 0; k + 1 < m; ++k) {
+            if ((rc = apply(m + k, pl.st))) return rc;
+            if ((rc = qr_step(w, pl, w.W1(), w.dp(k), w.Tpi(k), w.Up(k + 1), w.dp(k + 1), w.Tpi(k + 1), nullptr)))
+                return rc;
+        }
+        EPHMC_CUDA(cudaEventRecord(w.ev[1], pl.st));
+    }
+    // Q side, top down, on the context's stream: U_{m-1} = 1, d = 1, T^-1 = 1
     k_eye<<<blocks(VV), 256, 0, st>>>(w.U(m - 1), V);
     k_eye<<<blocks(VV), 256, 0, st>>>(w.Ti(m - 1), V);
-    k_ones<<<blocks(V), 256, 0, st>>>(w.d(m - 1), V, w.info);
+    k_ones<<<blocks(V), 256, 0, st>>>(w.d(m - 1), V, q.info);
     count_launch(3);
     for (int k = m - 1; k >= 0; --k) {
-        if ((rc = apply(m - 1 - k))) return rc;
-        if (k >= 1 && (rc = qr_step(w, w.SU(k), w.d(k), w.Ti(k), w.U(k - 1), w.d(k - 1), w.Ti(k - 1), w.info, st)))
+        if ((rc = apply(m - 1 - k, st))) return rc;
+        if (k >= 1 && (rc = qr_step(w, q, w.SU(k), w.d(k), w.Ti(k), w.U(k - 1), w.d(k - 1), w.Ti(k - 1), q.info)))
             return rc;
     }
-    const double one = 1.0, zero = 0.0;
     // log det: one more step absorbs S_0, the whole product = U diag(d) T
-    // (U in W, T^-1 in yst(m-1), d in the norms' slot, all free until the
-    // P side), and 1 + U D T = U N D_b T with N = U^T T^-1 D_b^-1 + D_s, so
+    // (U in W, T^-1 in yst(m-1), d in its own slot), and 1 + U D T =
+    // U N D_b T with N = U^T T^-1 D_b^-1 + D_s, so
     // log|det M| = log|det N| + sum log d_b, sign = sign det(U N T)
     {
         double *Uw = w.W(), *Tw = w.yst(m - 1), *dw = w.dwhole();
-        if ((rc = qr_step(w, w.SU(0), w.d(0), w.Ti(0), Uw, dw, Tw, w.info, st, true))) return rc;
-        STAB_BLAS(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_N, V, V, V, &one, Uw, V, Tw, V, &zero, w.N(), V));
+        if ((rc = qr_step(w, q, w.SU(0), w.d(0), w.Ti(0), Uw, dw, Tw, q.info, true))) return rc;
+        STAB_BLAS(cublasDgemm(q.blas, CUBLAS_OP_T, CUBLAS_OP_N, V, V, V, &one, Uw, V, Tw, V, &zero, w.N(), V));
         k_form_N_whole<<<blocks(VV), 256, 0, st>>>(w.N(), dw, V);
         count_launch(2);
-        STAB_SOLVER(cusolverDnDgetrf(w.sol, V, V, w.N(), V, w.ws, w.piv(), w.info));
-        k_logdet_parts<<<1, 1024, 0, st>>>(w.N(), w.piv(), dw, w.info, V, w.parts());
+        STAB_SOLVER(cusolverDnDgetrf(q.sol, V, V, w.N(), V, q.ws, w.piv(), q.info));
+        k_logdet_parts<<<1, 1024, 0, st>>>(w.N(), w.piv(), dw, q.info, V, w.parts());
         count_launch(1);
-    }
-    // k = 0: N_0 = T_0^-1 D_b^-1 + S_0 U_0 D_s (U', d', T' = 1)
-    {
-        k_ones<<<blocks(V), 256, 0, st>>>(w.dp(0), V, nullptr);
-        count_launch(1);
-        if (want_z) {
-            EPHMC_CUDA(cudaMemcpyAsync(w.N(), w.Ti(0), sizeof(double) * VV, cudaMemcpyDeviceToDevice, st));
-            k_form_N<<<blocks(VV), 256, 0, st>>>(w.N(), w.SU(0), w.d(0), w.dp(0), V);
-            count_launch(1);
-            STAB_SOLVER(cusolverDnDgetrf(w.sol, V, V, w.N(), V, w.ws, w.piv(), w.info));
-            // Z_0 = U_0 D_s N_0^-1 (U', D' = 1): y start of the bottom segment
-            k_eye<<<blocks(VV), 256, 0, st>>>(w.W(), V);
-            count_launch(1);
-            STAB_SOLVER(cusolverDnDgetrs(w.sol, CUBLAS_OP_N, V, V, w.N(), V, w.piv(), w.W(), V, w.info));
-            k_scale_rows_small<<<blocks(VV), 256, 0, st>>>(w.W(), w.d(0), V);
-            count_launch(2);
-            STAB_BLAS(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_T, V, V, V, &one, w.W(), V, w.U(0), V, &zero,
-                                  w.yst(m - 1), V));
-            count_launch(1);
-        }
     }
     if (!want_z) {
         EPHMC_CUDA(cudaGetLastError());
         return EPHMC_OK;
     }
-    // P side, bottom up: U'_0 = 1, d' = 1, T'^-1 = 1
-    k_eye<<<blocks(VV), 256, 0, st>>>(w.Up(0), V);
-    k_eye<<<blocks(VV), 256, 0, st>>>(w.Tpi(0), V);
+    EPHMC_CUDA(cudaStreamWaitEvent(st, w.ev[1], 0));  // join the P side
+    // Z_0 = U_0 D_s N_0^-1 with N_0 = T_0^-1 D_b^-1 + S_0 U_0 D_s (U', d', T' = 1):
+    // y start of the bottom segment
+    EPHMC_CUDA(cudaMemcpyAsync(w.N(), w.Ti(0), sizeof(double) * VV, cudaMemcpyDeviceToDevice, st));
+    k_form_N<<<blocks(VV), 256, 0, st>>>(w.N(), w.SU(0), w.d(0), w.dp(0), V);
+    count_launch(1);
+    STAB_SOLVER(cusolverDnDgetrf(q.sol, V, V, w.N(), V, q.ws, w.piv(), q.info));
+    k_eye<<<blocks(VV), 256, 0, st>>>(w.W(), V);
+    count_launch(1);
+    STAB_SOLVER(cusolverDnDgetrs(q.sol, CUBLAS_OP_N, V, V, w.N(), V, w.piv(), w.W(), V, q.info));
+    k_scale_rows_small<<<blocks(VV), 256, 0, st>>>(w.W(), w.d(0), V);
     count_launch(2);
-    for (int k = 0; k + 1 < m; ++k) {
-        if ((rc = apply(m + k))) return rc;  // W = S_k^T U'_k
-        if ((rc = qr_step(w, w.W(), w.dp(k), w.Tpi(k), w.Up(k + 1), w.dp(k + 1), w.Tpi(k + 1), nullptr, st)))
-            return rc;
-    }
+    STAB_BLAS(cublasDgemm(q.blas, CUBLAS_OP_T, CUBLAS_OP_T, V, V, V, &one, w.W(), V, w.U(0), V, &zero, w.yst(m - 1),
+                          V));
+    count_launch(1);
     // Z_k, k = 1..m-1
     for (int k = 1; k < m; ++k) {
-        STAB_BLAS(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_N, V, V, V, &one, w.Tpi(k), V, w.Ti(k), V, &zero, w.N(),
+        STAB_BLAS(cublasDgemm(q.blas, CUBLAS_OP_T, CUBLAS_OP_N, V, V, V, &one, w.Tpi(k), V, w.Ti(k), V, &zero, w.N(),
                               V));
-        STAB_BLAS(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_N, V, V, V, &one, w.Up(k), V, w.SU(k), V, &zero, w.W(),
+        STAB_BLAS(cublasDgemm(q.blas, CUBLAS_OP_T, CUBLAS_OP_N, V, V, V, &one, w.Up(k), V, w.SU(k), V, &zero, w.W(),
                               V));
         k_form_N<<<blocks(VV), 256, 0, st>>>(w.N(), w.W(), w.d(k), w.dp(k), V);
-        STAB_SOLVER(cusolverDnDgetrf(w.sol, V, V, w.N(), V, w.ws, w.piv(), w.info));
+        STAB_SOLVER(cusolverDnDgetrf(q.sol, V, V, w.N(), V, q.ws, w.piv(), q.info));
         k_rhs<<<blocks(VV), 256, 0, st>>>(w.Up(k), w.dp(k), V, w.W());
-        STAB_SOLVER(cusolverDnDgetrs(w.sol, CUBLAS_OP_N, V, V, w.N(), V, w.piv(), w.W(), V, w.info));
+        STAB_SOLVER(cusolverDnDgetrs(q.sol, CUBLAS_OP_N, V, V, w.N(), V, w.piv(), w.W(), V, q.info));
         k_scale_rows_small<<<blocks(VV), 256, 0, st>>>(w.W(), w.d(k), V);
-        STAB_BLAS(cublasDgemm(w.blas, CUBLAS_OP_T, CUBLAS_OP_T, V, V, V, &one, w.W(), V, w.U(k), V, &zero,
+        STAB_BLAS(cublasDgemm(q.blas, CUBLAS_OP_T, CUBLAS_OP_T, V, V, V, &one, w.W(), V, w.U(k), V, &zero,
                               w.yst(m - 1 - k), V));
         count_launch(8);
     }
