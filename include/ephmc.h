@@ -198,9 +198,10 @@ EPHMC_API int ephmc_ctx_set_checkpoint(ephmc_ctx *ctx, unsigned interval);
  * Z = Q_{t1-1} M^-1 P_{t0} in FP64 (sweep 1's state at the segment top, an
  * FP64 y chain and one GEMM per segment) and only the in-segment products
  * L_t, R_t in FP32, so the FP32 sums cancel over one segment's growth instead
- * of the whole chain's.  0 restores the built-in length, min(Nt, 16).  With
- * checkpointing (ephmc_ctx_set_checkpoint) the checkpoint interval is the
- * segment length. */
+ * of the whole chain's.  0 restores the built-in length, min(16, max(1, Nt/4)).
+ * With checkpointing (ephmc_ctx_set_checkpoint) the checkpoint interval is the
+ * segment length.  A stabilised context (ephmc_ctx_set_stabilize) cuts its
+ * chain into segments of `length` slices, by default min(6, max(1, Nt/4)). */
 EPHMC_API int ephmc_ctx_set_segment(ephmc_ctx *ctx, unsigned length);
 /* No counterpart in the reference.  on != 0: the adjoint and mixed forces
  * (and their log det) come from an FP64 re-stabilised slice chain, for low
