@@ -435,7 +435,9 @@ int ensure_seg(ephmc_ctx *c, const SegPlan &p) {
 // the packed FP32 strip kernel where it applies, else the FP64 slice kernel
 // with an FP32 stack
 int launch_identity_stacks(ephmc_ctx *c, const double *x, const SliceJob *jobs_dev, int n) {
-    if (slices_strip_supported(c->lat)) return launch_slices_strip_identity_f32(x, c->c, c->lat, jobs_dev, n, c->stream);
+    if (slices_strip32_supported(c->lat))
+        return launch_slices_strip_identity_f32(x, c->c, c->lat, jobs_dev, n, c->stream);
+    if (slices_tile_supported(c->lat)) return launch_slices_tile<float>(x, c->c, c->lat, jobs_dev, n, c->stream);
     return launch_slices<double, double, float>(Axis::Rows, x, c->c, c->lat, jobs_dev, n, c->stream);
 }
 
@@ -487,7 +489,7 @@ int sweep1_seg(ephmc_ctx *c, const double *x, double *dst) {
     // before the force sweep reads them.
     const int lu_sms = c->V <= 1024 ? (int)((c->V + kLuPanel - 1) / kLuPanel) : c->sm_count;
     const int free_sms = c->sm_count - lu_sms;
-    if (!slices_strip_supported(c->lat) || free_sms < 8)
+    if (!slices_strip32_supported(c->lat) || free_sms < 8)
         return launch_identity_stacks(c, x, c->jobs + p.m, (int)id.size());
     EPHMC_CUDA(cudaEventRecord(c->aux_ev[0], c->stream));
     EPHMC_CUDA(cudaStreamWaitEvent(c->aux_stream, c->aux_ev[0], 0));

@@ -170,16 +170,22 @@ template <typename Real, typename Store, typename StackT>
 int launch_slices(Axis axis, const double *x, const Couplings &c, const LatticeDev &lat,
                   const SliceJob *jobs_dev, int njobs, cudaStream_t st);
 
-// Same jobs on rows (identity or src start, Rows axis only) for L1 = 32
-// lattices with the lattice in registers (slices_strip.cu); sums in a
-// different order from launch_slices, so results agree to rounding.
-bool slices_strip_supported(const LatticeDev &lat);
+// Same jobs on rows (identity or src start, Rows axis only) with the lattice
+// in registers: L1 = 32 (slices_strip.cu) and L1 = 8, 12, 16, 24, 48
+// (register tiles, slices_tile.cu); sums in a different order from
+// launch_slices, so results agree to rounding.
+bool slices_strip32_supported(const LatticeDev &lat);
+bool slices_tile_supported(const LatticeDev &lat);
+bool slices_strip_supported(const LatticeDev &lat);  // either of the two
 template <typename StackT>
 int launch_slices_strip(const double *x, const Couplings &c, const LatticeDev &lat, const SliceJob *jobs_dev,
                         int njobs, cudaStream_t st);
+template <typename StackT>
+int launch_slices_tile(const double *x, const Couplings &c, const LatticeDev &lat, const SliceJob *jobs_dev,
+                       int njobs, cudaStream_t st);
 // FP32 (packed pairs) for jobs that start from the identity and spill every
 // state, the last included, to an FP32 stack (dst null): the segmented mixed
-// force's stacks (slices_strip.cu).  max_ctas > 0 caps the grid (the work is
+// force's stacks (slices_strip.cu; L1 = 32).  max_ctas > 0 caps the grid (the work is
 // taken grid-stride), so that the launch can run on the SMs the LU leaves free.
 int launch_slices_strip_identity_f32(const double *x, const Couplings &c, const LatticeDev &lat,
                                      const SliceJob *jobs_dev, int njobs, cudaStream_t st, int max_ctas = 0);

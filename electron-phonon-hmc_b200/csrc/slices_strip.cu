@@ -187,14 +187,16 @@ int launch_strip(const double *x, const Couplings &c, const LatticeDev &lat, con
 
 }  // namespace
 
-bool slices_strip_supported(const LatticeDev &lat) {
+bool slices_strip32_supported(const LatticeDev &lat) {
     return lat.l1 == 32 && lat.l2 >= 4 && lat.l2 % 4 == 0 && lat.l2 / 4 <= 8;
 }
+
+bool slices_strip_supported(const LatticeDev &lat) { return slices_strip32_supported(lat) || slices_tile_supported(lat); }
 
 template <typename StackT>
 int launch_slices_strip(const double *x, const Couplings &c, const LatticeDev &lat, const SliceJob *jobs_dev,
                         int njobs, cudaStream_t st) {
-    if (!slices_strip_supported(lat)) return EPHMC_ERR_UNSUPPORTED;
+    if (!slices_strip32_supported(lat)) return launch_slices_tile<StackT>(x, c, lat, jobs_dev, njobs, st);
     if (njobs <= 0) return EPHMC_OK;
     return launch_strip<StackT, 2, 4>(x, c, lat, jobs_dev, njobs, st);
 }
@@ -353,7 +355,7 @@ __global__ void __launch_bounds__(512, 1) k_slices_strip_f32(const double *__res
 
 int launch_slices_strip_identity_f32(const double *x, const Couplings &c, const LatticeDev &lat,
                                      const SliceJob *jobs_dev, int njobs, cudaStream_t st, int max_ctas) {
-    if (!slices_strip_supported(lat)) return EPHMC_ERR_UNSUPPORTED;
+    if (!slices_strip32_supported(lat)) return EPHMC_ERR_UNSUPPORTED;
     if (njobs <= 0) return EPHMC_OK;
     constexpr int H = 4, G = 2;
     const int V = lat.V, L2 = lat.l2, nw = L2 / H;

@@ -37,3 +37,33 @@ def test_strip_sweep_adjoint_matches_reference_path(gpu, restated, l2, nt, beta)
     # measured: adjoint 2e-15, mixed 7e-7 on all three shapes
     assert err_a <= 1e-12
     assert err_m <= 1e-5
+
+
+# Register-tile layouts of the same sweep for L1 != 32 (slices_tile.cu): L1 =
+# 48 (3 columns per lane, 16 lanes per row), 24 (3 columns, 8 lanes), 16 and
+# 12 (one column, 16 lanes; 12 of them hold sites), 8 (one column, 8 lanes).
+TILE_SHAPES = [(48, 4, 8, 2.0), (48, 48, 16, 4.0), (24, 8, 8, 2.0), (24, 24, 16, 4.0), (16, 16, 16, 4.0),
+               (12, 12, 16, 4.0), (8, 8, 16, 4.0), (8, 24, 8, 2.0)]
+
+
+@pytest.mark.parametrize("l1,l2,nt,beta", TILE_SHAPES)
+def test_tile_sweep_adjoint_matches_reference_path(gpu, restated, l1, l2, nt, beta):
+    """Sweep 1, the y chain and the segment stacks of the adjoint and mixed
+    paths run the register-tile kernel on these lattices; the reference path
+    keeps the reference's summation order.  Log det to 1e-12, the FP64
+    adjoint force to 1e-12 and the mixed force to 1e-5 of the reference
+    path's."""
+    import ephmc
+    from oracle import Model
+    m = Model.physical(l1, l2, nt, beta)
+    x = restated.random_x(7, m.dim)
+    with ephmc.Context(l1, l2, nt, m.t, m.kappa, m.mu, m.omega) as ctx:
+        ld_r, pd_r = ctx.eval(x, mode="reference")
+        ld_a, pd_a = ctx.eval(x, mode="adjoint")
+        ld_m, pd_m = ctx.eval(x, mode="mixed")
+    err_a, err_m = rel(pd_a, pd_r), rel(pd_m, pd_r)
+    print(f"{l1}x{l2} Nt={nt}: log det {ld_a - ld_r:.2e}, adjoint {err_a:.2e}, mixed {err_m:.2e}")
+    assert abs(ld_a - ld_r) <= 1e-12 * abs(ld_r) + 1e-12
+    assert abs(ld_m - ld_r) <= 1e-12 * abs(ld_r) + 1e-12
+    assert err_a <= 1e-12
+    assert err_m <= 1e-5
