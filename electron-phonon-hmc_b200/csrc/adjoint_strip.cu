@@ -317,14 +317,20 @@ __global__ void __launch_bounds__(512, 1) k_adjoint_strip(const double *__restri
 
 }  // namespace
 
-bool adjoint_strip_supported(const LatticeDev &lat) {
+bool adjoint_strip32_supported(const LatticeDev &lat) {
     return lat.l1 == 32 && lat.l2 >= kH && lat.l2 % kH == 0 && kG * (lat.l2 / kH) * 32 <= 512;
+}
+
+bool adjoint_strip_supported(const LatticeDev &lat) {
+    return adjoint_strip32_supported(lat) || adjoint_tile_supported(lat);
 }
 
 int launch_adjoint_strip(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
                          double *force, cudaStream_t st, const AdjointRange *range, int seg_count) {
-    if (!adjoint_strip_supported(lat)) return EPHMC_ERR_UNSUPPORTED;
+    if (!adjoint_strip32_supported(lat))
+        return launch_adjoint_tile(x, c, lat, qstack, Minv, nt, flavors, single_particle, logdet, force, st, range,
+                                   seg_count);
     const int V = lat.V, L2 = lat.l2, nw = L2 / kH;
     const size_t smem = sizeof(float) * (6 * (size_t)V + 2 * (size_t)kG * kSlots * kR * nw * 32);
     if (smem > 227 * 1024) return EPHMC_ERR_UNSUPPORTED;

@@ -437,7 +437,7 @@ int ensure_seg(ephmc_ctx *c, const SegPlan &p) {
 int launch_identity_stacks(ephmc_ctx *c, const double *x, const SliceJob *jobs_dev, int n) {
     if (slices_strip32_supported(c->lat))
         return launch_slices_strip_identity_f32(x, c->c, c->lat, jobs_dev, n, c->stream);
-    if (slices_tile_supported(c->lat)) return launch_slices_tile<float>(x, c->c, c->lat, jobs_dev, n, c->stream);
+    if (slices_tile_supported(c->lat)) return launch_slices_tile_identity_f32(x, c->c, c->lat, jobs_dev, n, c->stream);
     return launch_slices<double, double, float>(Axis::Rows, x, c->c, c->lat, jobs_dev, n, c->stream);
 }
 

@@ -183,6 +183,10 @@ int launch_slices_strip(const double *x, const Couplings &c, const LatticeDev &l
 template <typename StackT>
 int launch_slices_tile(const double *x, const Couplings &c, const LatticeDev &lat, const SliceJob *jobs_dev,
                        int njobs, cudaStream_t st);
+// jobs from the identity with FP32 stacks and no destination, in FP32
+// arithmetic (the mixed force's segment stacks on the tile lattices)
+int launch_slices_tile_identity_f32(const double *x, const Couplings &c, const LatticeDev &lat,
+                                    const SliceJob *jobs_dev, int njobs, cudaStream_t st);
 // FP32 (packed pairs) for jobs that start from the identity and spill every
 // state, the last included, to an FP32 stack (dst null): the segmented mixed
 // force's stacks (slices_strip.cu; L1 = 32).  max_ctas > 0 caps the grid (the work is
@@ -207,9 +211,14 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
                          int single_particle, double logdet, double *force, cudaStream_t st,
                          const AdjointRange *range = nullptr, int seg_count = 1);
 
-// FP32 adjoint sweep 2 for L1 = 32 lattices with the lattice in registers
-// (adjoint_strip.cu)
-bool adjoint_strip_supported(const LatticeDev &lat);
+// FP32 adjoint sweep 2 with the lattice in registers: L1 = 32 (adjoint_strip.cu)
+// and the register-tile lattices L1 = 8, 12, 16, 24 (adjoint_tile.cu)
+bool adjoint_strip32_supported(const LatticeDev &lat);
+bool adjoint_tile_supported(const LatticeDev &lat);
+bool adjoint_strip_supported(const LatticeDev &lat);  // either of the two
+int launch_adjoint_tile(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
+                        const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
+                        double *force, cudaStream_t st, const AdjointRange *range = nullptr, int seg_count = 1);
 int launch_adjoint_strip(const double *x, const Couplings &c, const LatticeDev &lat, const float *qstack,
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
                          double *force, cudaStream_t st, const AdjointRange *range = nullptr,

@@ -27,24 +27,23 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-struct HopT {
-    double f0, f1, f2, f0l, f1d, f2dr;
+template <typename Real> struct HopT {
+    Real f0, f1, f2, f0l, f1d, f2dr;
 };
 
 // (H v)(a, b) = mu v + f0 v(a+1,b) + f0(a-1,b) v(a-1,b) + f1 v(a,b+1)
 //             + f1(a,b-1) v(a,b-1) + f2 v(a-1,b+1) + f2(a+1,b-1) v(a+1,b-1),
 // in the summation order of the L1 = 32 strip kernel
-__device__ __forceinline__ double stencil_t(const HopT &h, double mu, double v, double l, double r, double up,
-                                            double down, double upleft, double downright) {
-    const double s1 = fma(h.f0, r, mu * v);
-    const double s2 = fma(h.f1, up, h.f0l * l);
-    const double s3 = fma(h.f2, upleft, h.f1d * down);
+template <typename Real>
+__device__ __forceinline__ Real stencil_t(const HopT<Real> &h, Real mu, Real v, Real l, Real r, Real up, Real down,
+                                          Real upleft, Real downright) {
+    const Real s1 = fma(h.f0, r, mu * v);
+    const Real s2 = fma(h.f1, up, h.f0l * l);
+    const Real s3 = fma(h.f2, upleft, h.f1d * down);
     return (s1 + s2) + fma(h.f2dr, downright, s3);
 }
 
-template <typename T> __device__ __forceinline__ void st_t(T *p, double v);
-template <> __device__ __forceinline__ void st_t<double>(double *p, double v) { *p = v; }
-template <> __device__ __forceinline__ void st_t<float>(float *p, double v) { *p = (float)v; }
+template <typename T, typename Real> __device__ __forceinline__ void st_t(T *p, Real v) { *p = (T)v; }
 
 // Thread geometry of the tile layout
 struct Tile {
@@ -74,10 +73,10 @@ __device__ __forceinline__ Tile tile_of(int L1, int L2) {
 
 // w = (mu + K) v for the thread's H x W sites of R vectors; the strips' bottom
 // and top rows through shared memory (edge[2][R][NS][L1])
-template <int R, int H, int W>
-__device__ __forceinline__ void apply_H_tile(const double (&v)[R][H][W], double (&w)[R][H][W],
-                                             const HopT (&hp)[H][W], double mu, double *edge, const Tile &t) {
-    double *bot = edge, *top = edge + (size_t)R * t.NS * t.L1;
+template <typename Real, int R, int H, int W>
+__device__ __forceinline__ void apply_H_tile(const Real (&v)[R][H][W], Real (&w)[R][H][W],
+                                             const HopT<Real> (&hp)[H][W], Real mu, Real *edge, const Tile &t) {
+    Real *bot = edge, *top = edge + (size_t)R * t.NS * t.L1;
     if (t.act) {
 #pragma unroll
         for (int r = 0; r < R; ++r)
@@ -91,48 +90,51 @@ __device__ __forceinline__ void apply_H_tile(const double (&v)[R][H][W], double 
     const int sb = t.s == 0 ? t.NS - 1 : t.s - 1, sa = t.s + 1 == t.NS ? 0 : t.s + 1;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        double dn[W], upx[W];
+        Real dn[W], upx[W];
 #pragma unroll
         for (int c = 0; c < W; ++c) {
             dn[c] = top[((size_t)r * t.NS + sb) * t.L1 + t.a0 + c];   // row b0 - 1
             upx[c] = bot[((size_t)r * t.NS + sa) * t.L1 + t.a0 + c];  // row b0 + H
         }
-        double Lh[H], Rh[H];  // (a0 - 1, b0 + h), (a0 + W, b0 + h)
+        Real Lh[H], Rh[H];  // (a0 - 1, b0 + h), (a0 + W, b0 + h)
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             Lh[h] = __shfl_sync(kFull, v[r][h][W - 1], t.lm);
             Rh[h] = __shfl_sync(kFull, v[r][h][0], t.lp);
         }
-        const double upL = __shfl_sync(kFull, upx[W - 1], t.lm);  // (a0 - 1, b0 + H)
-        const double dnR = __shfl_sync(kFull, dn[0], t.lp);       // (a0 + W, b0 - 1)
+        const Real upL = __shfl_sync(kFull, upx[W - 1], t.lm);  // (a0 - 1, b0 + H)
+        const Real dnR = __shfl_sync(kFull, dn[0], t.lp);       // (a0 + W, b0 - 1)
 #pragma unroll
         for (int h = 0; h < H; ++h)
 #pragma unroll
             for (int c = 0; c < W; ++c) {
-                const double l = c > 0 ? v[r][h][c - 1] : Lh[h];
-                const double rt = c + 1 < W ? v[r][h][c + 1] : Rh[h];
-                const double up = h + 1 < H ? v[r][h + 1][c] : upx[c];
-                const double down = h > 0 ? v[r][h - 1][c] : dn[c];
-                const double ul = h + 1 < H ? (c > 0 ? v[r][h + 1][c - 1] : Lh[h + 1]) : (c > 0 ? upx[c - 1] : upL);
-                const double dr = h > 0 ? (c + 1 < W ? v[r][h - 1][c + 1] : Rh[h - 1]) : (c + 1 < W ? dn[c + 1] : dnR);
-                w[r][h][c] = stencil_t(hp[h][c], mu, v[r][h][c], l, rt, up, down, ul, dr);
+                const Real l = c > 0 ? v[r][h][c - 1] : Lh[h];
+                const Real rt = c + 1 < W ? v[r][h][c + 1] : Rh[h];
+                const Real up = h + 1 < H ? v[r][h + 1][c] : upx[c];
+                const Real down = h > 0 ? v[r][h - 1][c] : dn[c];
+                const Real ul = h + 1 < H ? (c > 0 ? v[r][h + 1][c - 1] : Lh[h + 1]) : (c > 0 ? upx[c - 1] : upL);
+                const Real dr = h > 0 ? (c + 1 < W ? v[r][h - 1][c + 1] : Rh[h - 1]) : (c + 1 < W ? dn[c + 1] : dnR);
+                w[r][h][c] = stencil_t<Real>(hp[h][c], mu, v[r][h][c], l, rt, up, down, ul, dr);
             }
     }
     __syncthreads();  // the edge buffer is reused by the next stencil
 }
 
-template <typename StackT, int R, int H, int W, int LPR, int MAXT>
+// Real: the arithmetic (double; float for stacks that start from the
+// identity and only feed the mixed force, as in the L1 = 32 FP32 kernel)
+template <typename Real, typename StackT, int R, int H, int W, int LPR, int MAXT>
 __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__ x, Couplings cp,
                                                       const SliceJob *__restrict__ jobs, int L1, int L2) {
-    extern __shared__ double edge_t[];  // [2][R][NS][L1]
+    extern __shared__ __align__(16) unsigned char smem_t[];
+    Real *edge_t = reinterpret_cast<Real *>(smem_t);  // [2][R][NS][L1]
     const SliceJob job = jobs[blockIdx.y];
     const Tile t = tile_of<W, LPR, H>(L1, L2);
     const int V = L1 * L2;
     const size_t VV = (size_t)V * V;
     const int vec0 = blockIdx.x * R;
-    const double mu = cp.mu;
+    const Real mu = (Real)cp.mu;
 
-    double v[R][H][W], w[R][H][W];
+    Real v[R][H][W], w[R][H][W];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int c = vec0 + r;
@@ -141,8 +143,8 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
 #pragma unroll
             for (int k = 0; k < W; ++k) {
                 const int i = (t.b0 + h) * L1 + t.a0 + k;
-                if (job.src == nullptr) v[r][h][k] = (t.act && c < V && i == c) ? 1.0 : 0.0;
-                else v[r][h][k] = (t.act && c < V) ? static_cast<const double *>(job.src)[(size_t)c * V + i] : 0.0;
+                if (job.src == nullptr) v[r][h][k] = (t.act && c < V && i == c) ? Real(1) : Real(0);
+                else v[r][h][k] = (t.act && c < V) ? (Real) static_cast<const double *>(job.src)[(size_t)c * V + i] : Real(0);
             }
     }
     const int bd = t.b0 == 0 ? L2 - 1 : t.b0 - 1;  // the row below the strip
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
         const double *xs = x + (size_t)sl * 3 * V;
         // hopping coefficients of the thread's sites and of the neighbours
         // they take from (left: link 0, below: link 1, below right: link 2)
-        HopT hp[H][W];
+        HopT<Real> hp[H][W];
 #pragma unroll
         for (int h = 0; h < H; ++h)
 #pragma unroll
@@ -159,20 +161,20 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
                 const int a = t.a0 + k, b = t.b0 + h;
                 const int al = a == 0 ? L1 - 1 : a - 1, ar = a + 1 == L1 ? 0 : a + 1;
                 const int bb = h > 0 ? b - 1 : bd;
-                hp[h][k].f0 = fma(-cp.kappa[0], __ldg(xs + 3 * (b * L1 + a) + 0), cp.t[0]);
-                hp[h][k].f1 = fma(-cp.kappa[1], __ldg(xs + 3 * (b * L1 + a) + 1), cp.t[1]);
-                hp[h][k].f2 = fma(-cp.kappa[2], __ldg(xs + 3 * (b * L1 + a) + 2), cp.t[2]);
-                hp[h][k].f0l = fma(-cp.kappa[0], __ldg(xs + 3 * (b * L1 + al) + 0), cp.t[0]);
-                hp[h][k].f1d = fma(-cp.kappa[1], __ldg(xs + 3 * (bb * L1 + a) + 1), cp.t[1]);
-                hp[h][k].f2dr = fma(-cp.kappa[2], __ldg(xs + 3 * (bb * L1 + ar) + 2), cp.t[2]);
+                hp[h][k].f0 = (Real)fma(-cp.kappa[0], __ldg(xs + 3 * (b * L1 + a) + 0), cp.t[0]);
+                hp[h][k].f1 = (Real)fma(-cp.kappa[1], __ldg(xs + 3 * (b * L1 + a) + 1), cp.t[1]);
+                hp[h][k].f2 = (Real)fma(-cp.kappa[2], __ldg(xs + 3 * (b * L1 + a) + 2), cp.t[2]);
+                hp[h][k].f0l = (Real)fma(-cp.kappa[0], __ldg(xs + 3 * (b * L1 + al) + 0), cp.t[0]);
+                hp[h][k].f1d = (Real)fma(-cp.kappa[1], __ldg(xs + 3 * (bb * L1 + a) + 1), cp.t[1]);
+                hp[h][k].f2dr = (Real)fma(-cp.kappa[2], __ldg(xs + 3 * (bb * L1 + ar) + 2), cp.t[2]);
             }
         for (int p = job.p_begin; p != job.p_end; p += job.p_step) {
             // p is 0 or 1; selecting avoids indexing the parameter struct at run time
-            const double al = p ? cp.a_lin[1] : cp.a_lin[0], aq = p ? cp.a_quad[1] : cp.a_quad[0];
-            apply_H_tile<R, H, W>(v, w, hp, mu, edge_t, t);
+            const Real al = (Real)(p ? cp.a_lin[1] : cp.a_lin[0]), aq = (Real)(p ? cp.a_quad[1] : cp.a_quad[0]);
+            apply_H_tile<Real, R, H, W>(v, w, hp, mu, edge_t, t);
             if (p ? cp.cplx[1] : cp.cplx[0]) {
-                double z[R][H][W];
-                apply_H_tile<R, H, W>(w, z, hp, mu, edge_t, t);
+                Real z[R][H][W];
+                apply_H_tile<Real, R, H, W>(w, z, hp, mu, edge_t, t);
 #pragma unroll
                 for (int r = 0; r < R; ++r)
 #pragma unroll
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
 #pragma unroll
             for (int k = 0; k < W; ++k) {
                 const int i = (t.b0 + h) * L1 + t.a0 + k;
-                dst[(size_t)c * V + i] = v[r][h][k] + ((job.add_identity && i == c) ? 1.0 : 0.0);
+                dst[(size_t)c * V + i] = (double)v[r][h][k] + ((job.add_identity && i == c) ? 1.0 : 0.0);
             }
     }
 }
@@ -240,17 +242,17 @@ bool tile_shape(int L1, int L2, TileShape &s) {
     return threads >= 32 && threads <= s.maxT && smem <= 48 * 1024;
 }
 
-template <typename StackT, int R, int H, int W, int LPR, int MAXT>
+template <typename Real, typename StackT, int R, int H, int W, int LPR, int MAXT>
 int launch_tile(const double *x, const Couplings &c, const LatticeDev &lat, const SliceJob *jobs, int njobs,
                 cudaStream_t st) {
     constexpr int G = 32 / LPR;
     const int V = lat.V, L1 = lat.l1, L2 = lat.l2, NS = L2 / H;
     const int threads = 32 * NS / G;
     if (threads > MAXT) return EPHMC_ERR_UNSUPPORTED;
-    const size_t smem = sizeof(double) * 2 * R * (size_t)NS * L1;
+    const size_t smem = sizeof(Real) * 2 * R * (size_t)NS * L1;
     if (smem > 48 * 1024) return EPHMC_ERR_UNSUPPORTED;
     dim3 grid((V + R - 1) / R, njobs);
-    k_slices_tile<StackT, R, H, W, LPR, MAXT><<<grid, threads, smem, st>>>(x, c, jobs, L1, L2);
+    k_slices_tile<Real, StackT, R, H, W, LPR, MAXT><<<grid, threads, smem, st>>>(x, c, jobs, L1, L2);
     ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
     return EPHMC_OK;
@@ -270,11 +272,27 @@ int launch_slices_tile(const double *x, const Couplings &c, const LatticeDev &la
     if (!tile_shape(lat.l1, lat.l2, s)) return EPHMC_ERR_UNSUPPORTED;
     if (njobs <= 0) return EPHMC_OK;
     switch (lat.l1) {
-    case 48: return launch_tile<StackT, 1, 1, 3, 16, 768>(x, c, lat, jobs_dev, njobs, st);
-    case 24: return launch_tile<StackT, 2, 1, 3, 8, 256>(x, c, lat, jobs_dev, njobs, st);
+    case 48: return launch_tile<double, StackT, 1, 1, 3, 16, 768>(x, c, lat, jobs_dev, njobs, st);
+    case 24: return launch_tile<double, StackT, 2, 1, 3, 8, 256>(x, c, lat, jobs_dev, njobs, st);
     case 16:
-    case 12: return launch_tile<StackT, 2, 2, 1, 16, 256>(x, c, lat, jobs_dev, njobs, st);
-    case 8: return launch_tile<StackT, 4, 2, 1, 8, 256>(x, c, lat, jobs_dev, njobs, st);
+    case 12: return launch_tile<double, StackT, 2, 2, 1, 16, 256>(x, c, lat, jobs_dev, njobs, st);
+    case 8: return launch_tile<double, StackT, 4, 2, 1, 8, 256>(x, c, lat, jobs_dev, njobs, st);
+    default: return EPHMC_ERR_UNSUPPORTED;
+    }
+}
+
+// Stacks from the identity in FP32 arithmetic (twice the vectors per CTA)
+int launch_slices_tile_identity_f32(const double *x, const Couplings &c, const LatticeDev &lat,
+                                    const SliceJob *jobs_dev, int njobs, cudaStream_t st) {
+    TileShape s;
+    if (!tile_shape(lat.l1, lat.l2, s)) return EPHMC_ERR_UNSUPPORTED;
+    if (njobs <= 0) return EPHMC_OK;
+    switch (lat.l1) {
+    case 48: return launch_tile<float, float, 2, 1, 3, 16, 768>(x, c, lat, jobs_dev, njobs, st);
+    case 24: return launch_tile<float, float, 4, 1, 3, 8, 256>(x, c, lat, jobs_dev, njobs, st);
+    case 16:
+    case 12: return launch_tile<float, float, 4, 2, 1, 16, 256>(x, c, lat, jobs_dev, njobs, st);
+    case 8: return launch_tile<float, float, 8, 2, 1, 8, 256>(x, c, lat, jobs_dev, njobs, st);
     default: return EPHMC_ERR_UNSUPPORTED;
     }
 }

@@ -49,10 +49,11 @@ TILE_SHAPES = [(48, 4, 8, 2.0), (48, 48, 16, 4.0), (24, 8, 8, 2.0), (24, 24, 16,
 @pytest.mark.parametrize("l1,l2,nt,beta", TILE_SHAPES)
 def test_tile_sweep_adjoint_matches_reference_path(gpu, restated, l1, l2, nt, beta):
     """Sweep 1, the y chain and the segment stacks of the adjoint and mixed
-    paths run the register-tile kernel on these lattices; the reference path
-    keeps the reference's summation order.  Log det to 1e-12, the FP64
-    adjoint force to 1e-12 and the mixed force to 1e-5 of the reference
-    path's."""
+    paths run the register-tile kernel on these lattices, and for L1 <= 24
+    the mixed force's sweep runs the register-tile adjoint (adjoint_tile.cu);
+    the reference path keeps the reference's summation order.  Log det to
+    1e-12, the FP64 adjoint force to 1e-12 and the mixed force to 1e-5 of the
+    reference path's."""
     import ephmc
     from oracle import Model
     m = Model.physical(l1, l2, nt, beta)
