@@ -236,21 +236,39 @@ __global__ void __launch_bounds__(MAXT, 1) k_adjoint_tile(const double *__restri
     for (int ts = rg.t0; ts < rg.t1; ++ts) {
         float *acc_t = acc + (ts & 1) * 3 * V;
         const double *xs = x + (size_t)ts * 3 * V;
+        // own links from x; the neighbours' from registers, the neighbouring
+        // lanes, or (the strip's bottom row) the row below
         HopS hp[H][W];
 #pragma unroll
         for (int h = 0; h < H; ++h)
 #pragma unroll
             for (int k = 0; k < W; ++k) {
-                const int a = t.a0 + k, b = t.b0 + h;
-                const int al = a == 0 ? L1 - 1 : a - 1, ar = a + 1 == L1 ? 0 : a + 1;
-                const int bb = h > 0 ? b - 1 : bd;
-                hp[h][k].f0 = (float)fma(-cp.kappa[0], __ldg(xs + 3 * (b * L1 + a) + 0), cp.t[0]);
-                hp[h][k].f1 = (float)fma(-cp.kappa[1], __ldg(xs + 3 * (b * L1 + a) + 1), cp.t[1]);
-                hp[h][k].f2 = (float)fma(-cp.kappa[2], __ldg(xs + 3 * (b * L1 + a) + 2), cp.t[2]);
-                hp[h][k].f0l = (float)fma(-cp.kappa[0], __ldg(xs + 3 * (b * L1 + al) + 0), cp.t[0]);
-                hp[h][k].f1d = (float)fma(-cp.kappa[1], __ldg(xs + 3 * (bb * L1 + a) + 1), cp.t[1]);
-                hp[h][k].f2dr = (float)fma(-cp.kappa[2], __ldg(xs + 3 * (bb * L1 + ar) + 2), cp.t[2]);
+                const double *xi = xs + 3 * ((t.b0 + h) * L1 + t.a0 + k);
+                hp[h][k].f0 = (float)fma(-cp.kappa[0], __ldg(xi + 0), cp.t[0]);
+                hp[h][k].f1 = (float)fma(-cp.kappa[1], __ldg(xi + 1), cp.t[1]);
+                hp[h][k].f2 = (float)fma(-cp.kappa[2], __ldg(xi + 2), cp.t[2]);
             }
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const float f0w = __shfl_sync(kFullA, hp[h][W - 1].f0, t.lm);
+#pragma unroll
+            for (int k = 0; k < W; ++k) hp[h][k].f0l = k > 0 ? hp[h][k - 1].f0 : f0w;
+        }
+#pragma unroll
+        for (int h = H - 1; h > 0; --h) {
+            const float f2e = __shfl_sync(kFullA, hp[h - 1][0].f2, t.lp);
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                hp[h][k].f1d = hp[h - 1][k].f1;
+                hp[h][k].f2dr = k + 1 < W ? hp[h - 1][k + 1].f2 : f2e;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int a = t.a0 + k, ar = a + 1 == L1 ? 0 : a + 1;
+            hp[0][k].f1d = (float)fma(-cp.kappa[1], __ldg(xs + 3 * (bd * L1 + a) + 1), cp.t[1]);
+            hp[0][k].f2dr = (float)fma(-cp.kappa[2], __ldg(xs + 3 * (bd * L1 + ar) + 2), cp.t[2]);
+        }
         // q(t): the stack entry t - t0, the segment's FP64 checkpoint (its last
         // slice, checkpointed evaluation), or e_c (slice nt-1; the top slice of
         // a segment of the grid)

@@ -151,23 +151,41 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
     for (int it = 0; it < job.s_count; ++it) {
         const int sl = job.s_first + it * job.s_dir;
         const double *xs = x + (size_t)sl * 3 * V;
-        // hopping coefficients of the thread's sites and of the neighbours
-        // they take from (left: link 0, below: link 1, below right: link 2)
+        // hopping coefficients of the thread's sites (its own links), and of
+        // the neighbours they take from (left: link 0, below: link 1, below
+        // right: link 2) from its registers, the neighbouring lanes, or, for
+        // the strip's bottom row, the row below
         HopT<Real> hp[H][W];
 #pragma unroll
         for (int h = 0; h < H; ++h)
 #pragma unroll
             for (int k = 0; k < W; ++k) {
-                const int a = t.a0 + k, b = t.b0 + h;
-                const int al = a == 0 ? L1 - 1 : a - 1, ar = a + 1 == L1 ? 0 : a + 1;
-                const int bb = h > 0 ? b - 1 : bd;
-                hp[h][k].f0 = (Real)fma(-cp.kappa[0], __ldg(xs + 3 * (b * L1 + a) + 0), cp.t[0]);
-                hp[h][k].f1 = (Real)fma(-cp.kappa[1], __ldg(xs + 3 * (b * L1 + a) + 1), cp.t[1]);
-                hp[h][k].f2 = (Real)fma(-cp.kappa[2], __ldg(xs + 3 * (b * L1 + a) + 2), cp.t[2]);
-                hp[h][k].f0l = (Real)fma(-cp.kappa[0], __ldg(xs + 3 * (b * L1 + al) + 0), cp.t[0]);
-                hp[h][k].f1d = (Real)fma(-cp.kappa[1], __ldg(xs + 3 * (bb * L1 + a) + 1), cp.t[1]);
-                hp[h][k].f2dr = (Real)fma(-cp.kappa[2], __ldg(xs + 3 * (bb * L1 + ar) + 2), cp.t[2]);
+                const double *xi = xs + 3 * ((t.b0 + h) * L1 + t.a0 + k);
+                hp[h][k].f0 = (Real)fma(-cp.kappa[0], __ldg(xi + 0), cp.t[0]);
+                hp[h][k].f1 = (Real)fma(-cp.kappa[1], __ldg(xi + 1), cp.t[1]);
+                hp[h][k].f2 = (Real)fma(-cp.kappa[2], __ldg(xi + 2), cp.t[2]);
             }
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const Real f0w = __shfl_sync(kFull, hp[h][W - 1].f0, t.lm);  // (a0 - 1, b)
+#pragma unroll
+            for (int k = 0; k < W; ++k) hp[h][k].f0l = k > 0 ? hp[h][k - 1].f0 : f0w;
+        }
+#pragma unroll
+        for (int h = H - 1; h > 0; --h) {
+            const Real f2e = __shfl_sync(kFull, hp[h - 1][0].f2, t.lp);  // (a0 + W, b - 1)
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                hp[h][k].f1d = hp[h - 1][k].f1;
+                hp[h][k].f2dr = k + 1 < W ? hp[h - 1][k + 1].f2 : f2e;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int a = t.a0 + k, ar = a + 1 == L1 ? 0 : a + 1;
+            hp[0][k].f1d = (Real)fma(-cp.kappa[1], __ldg(xs + 3 * (bd * L1 + a) + 1), cp.t[1]);
+            hp[0][k].f2dr = (Real)fma(-cp.kappa[2], __ldg(xs + 3 * (bd * L1 + ar) + 2), cp.t[2]);
+        }
         for (int p = job.p_begin; p != job.p_end; p += job.p_step) {
             // p is 0 or 1; selecting avoids indexing the parameter struct at run time
             const Real al = (Real)(p ? cp.a_lin[1] : cp.a_lin[0]), aq = (Real)(p ? cp.a_quad[1] : cp.a_quad[0]);
@@ -228,7 +246,7 @@ struct TileShape {
 
 bool tile_shape(int L1, int L2, TileShape &s) {
     switch (L1) {
-    case 48: s = {3, 16, 1, 1, 768}; break;
+    case 48: s = {3, 16, 2, 1, 384}; break;
     case 24: s = {3, 8, 1, 2, 256}; break;
     case 16: s = {1, 16, 2, 2, 256}; break;
     case 12: s = {1, 16, 2, 2, 256}; break;  // 12 of 16 lanes per row
@@ -272,7 +290,7 @@ int launch_slices_tile(const double *x, const Couplings &c, const LatticeDev &la
     if (!tile_shape(lat.l1, lat.l2, s)) return EPHMC_ERR_UNSUPPORTED;
     if (njobs <= 0) return EPHMC_OK;
     switch (lat.l1) {
-    case 48: return launch_tile<double, StackT, 1, 1, 3, 16, 768>(x, c, lat, jobs_dev, njobs, st);
+    case 48: return launch_tile<double, StackT, 1, 2, 3, 16, 384>(x, c, lat, jobs_dev, njobs, st);
     case 24: return launch_tile<double, StackT, 2, 1, 3, 8, 256>(x, c, lat, jobs_dev, njobs, st);
     case 16:
     case 12: return launch_tile<double, StackT, 2, 2, 1, 16, 256>(x, c, lat, jobs_dev, njobs, st);
@@ -288,7 +306,7 @@ int launch_slices_tile_identity_f32(const double *x, const Couplings &c, const L
     if (!tile_shape(lat.l1, lat.l2, s)) return EPHMC_ERR_UNSUPPORTED;
     if (njobs <= 0) return EPHMC_OK;
     switch (lat.l1) {
-    case 48: return launch_tile<float, float, 2, 1, 3, 16, 768>(x, c, lat, jobs_dev, njobs, st);
+    case 48: return launch_tile<float, float, 2, 2, 3, 16, 384>(x, c, lat, jobs_dev, njobs, st);
     case 24: return launch_tile<float, float, 4, 1, 3, 8, 256>(x, c, lat, jobs_dev, njobs, st);
     case 16:
     case 12: return launch_tile<float, float, 4, 2, 1, 16, 256>(x, c, lat, jobs_dev, njobs, st);
