@@ -587,6 +587,309 @@ __global__ void __launch_bounds__(MAXT, 1) k_gj_dataflow(double *__restrict__ M,
     }
 }
 
+// ---------------------------------------------------------------- two panels per CTA
+// The dataflow kernel for 1024 < V <= 2304, where one 8-column panel per CTA
+// would need more CTAs (V / 8 > 128) than the SMs hold at one per SM: CTA b
+// owns panel b in registers (5 rows per thread, 512 threads) and panel
+// b + nCTA in shared memory (8 x 2560 doubles, 160 KB), nCTA = ceil(P / 2)
+// for P = V / 8 panels.  The protocol is that of k_gj_dataflow: panels are
+// taken in order, the owner runs the 8 pivot steps on its block and
+// publishes the swept block, the pivots and U's diagonal with a ready flag
+// (per-call epoch, bounded waits), every other CTA applies the block update
+// A(O, c) += K(O, :) A(P, c), A(P, c) = K(P, :) A(P, c) to both of its panels.
+// The shared-memory panel's pivot steps index its columns directly instead of
+// rotating registers.  The update accumulates into the columns (pivot rows
+// first set to zero) two multipliers at a time.
+constexpr int kLu2Threads = 512, kLu2Rpt = 5;
+constexpr int kLu2MaxV = 2304;                   // 2 * 8 panel columns per SM on 144 SMs
+constexpr int kLu2Rows = kLu2Threads * kLu2Rpt;  // 2560 rows held (the last ones padding)
+
+__global__ void __launch_bounds__(kLu2Threads, 1) k_gj_dataflow2(double *__restrict__ M, int V,
+                                                                double *__restrict__ panels, int *__restrict__ ipiv,
+                                                                double *__restrict__ diag, int *__restrict__ info,
+                                                                unsigned *__restrict__ sync, int withhold) {
+    constexpr int NB = kLuPanel, RPT = kLu2Rpt, MW = kLu2Threads / 32, LD = kLu2Rows;
+    __shared__ unsigned long long ck[2][MW];
+    __shared__ int cl[2][MW], cphys[2][MW];
+    __shared__ double cval[2][MW];
+    __shared__ __align__(16) double crow[2][MW][NB];
+    __shared__ __align__(16) double CpA[2][NB][NB], CpB[2][NB][NB];  // [buf][q][m]: pivot row m, column q
+    __shared__ int s_ip[2][NB];
+    __shared__ int own_pA[NB], own_pB[NB];
+    __shared__ int s_abort;
+    __shared__ unsigned s_epoch;
+    __shared__ double s_l[MW];
+    __shared__ int s_n[MW];
+    extern __shared__ __align__(16) double sB[];  // [NB][LD]: the second panel
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, T = (int)blockDim.x, NW = T >> 5;
+    const int b = blockIdx.x, ncta = gridDim.x;
+    const int P = (V + NB - 1) / NB;
+    const int pA = b, pB = b + ncta;  // pB < P: the CTA has a second panel
+    const bool hasB = pB < P;
+    const int cA = pA * NB, ncolA = min(NB, V - cA), cB = pB * NB, ncolB = hasB ? min(NB, V - cB) : 0;
+    const int last_owner = P - 1 - ncta;  // the owner of panel P - 1 (as its second panel)
+    unsigned *ready = sync + 1;
+    int row[RPT], lpos[RPT];
+    double a[RPT][NB];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        row[i] = tid + i * T;
+        lpos[i] = row[i];
+#pragma unroll
+        for (int q = 0; q < NB; ++q) {
+            a[i][q] = (row[i] < V && q < ncolA) ? M[(size_t)(cA + q) * V + row[i]] : 0.0;
+            sB[q * LD + row[i]] = (row[i] < V && q < ncolB) ? M[(size_t)(cB + q) * V + row[i]] : 0.0;
+        }
+    }
+    if (tid == 0) {
+        s_abort = 0;
+        const unsigned e = __ldcg(sync) + 1u;
+        s_epoch = e ? e : 1u;
+    }
+    __syncthreads();
+    const unsigned epoch = s_epoch;
+
+    // the register panel and the shared-memory panel exchange places
+    auto swap_panels = [&]() {
+#pragma unroll
+        for (int i = 0; i < RPT; ++i)
+#pragma unroll
+            for (int q = 0; q < NB; ++q) {
+                const double t = sB[q * LD + row[i]];
+                sB[q * LD + row[i]] = a[i][q];
+                a[i][q] = t;
+            }
+    };
+
+    // Panel k's block update (its swept block K published at columns j0.. of
+    // panels) applied to this CTA's register panel (doA) and shared-memory
+    // panel (doB); the rows' logical positions already follow panel k.  Row
+    // by row: the row's K entries are read once and serve both panels; rows
+    // P start from zero (A(P, c) = K(P, :) A(P, c)), the others from their
+    // value (A(O, c) += K(O, :) A(P, c)).
+    auto apply_panel = [&](int k, int j0, int nbc, bool doA, bool doB) {
+        const int buf = k & 1;
+        bool is_p[RPT];
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+            is_p[i] = row[i] < V && lpos[i] >= j0 && lpos[i] < j0 + nbc;
+            if (is_p[i]) {
+                const int m = lpos[i] - j0;
+#pragma unroll
+                for (int q = 0; q < NB; ++q) {
+                    if (doA) CpA[buf][q][m] = a[i][q];
+                    if (doB) CpB[buf][q][m] = sB[q * LD + row[i]];
+                }
+            }
+        }
+        // a short last panel: the missing pivot rows are zero
+        for (int e = tid; nbc < NB && e < NB * NB; e += T)
+            if (e % NB >= nbc) {
+                CpA[buf][e / NB][e % NB] = 0.0;
+                CpB[buf][e / NB][e % NB] = 0.0;
+            }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+            if (row[i] >= V) continue;
+            double kr[NB];
+#pragma unroll
+            for (int m = 0; m < NB; ++m) kr[m] = m < nbc ? __ldcg(panels + (size_t)(j0 + m) * V + row[i]) : 0.0;
+            if (doA) {
+#pragma unroll
+                for (int q = 0; q < NB; ++q) {
+                    double acc = is_p[i] ? 0.0 : a[i][q];
+#pragma unroll
+                    for (int m = 0; m < NB; m += 2) {
+                        const double2 cp = *reinterpret_cast<const double2 *>(&CpA[buf][q][m]);
+                        acc = fma(kr[m + 1], cp.y, fma(kr[m], cp.x, acc));
+                    }
+                    a[i][q] = acc;
+                }
+            }
+            if (doB) {
+                double *col = sB + row[i];
+#pragma unroll
+                for (int q = 0; q < NB; ++q) {
+                    double acc = is_p[i] ? 0.0 : col[q * LD];
+#pragma unroll
+                    for (int m = 0; m < NB; m += 2) {
+                        const double2 cp = *reinterpret_cast<const double2 *>(&CpB[buf][q][m]);
+                        acc = fma(kr[m + 1], cp.y, fma(kr[m], cp.x, acc));
+                    }
+                    col[q * LD] = acc;
+                }
+            }
+        }
+    };
+
+    for (int k = 0; k < P; ++k) {
+        const int j0 = k * NB, nbc = min(NB, V - j0);
+        if (k == pA || k == pB) {
+            // the panel to factor in registers: the second panel trades places
+            // with the first for its 8 steps (each thread its own rows)
+            const bool second = (k == pB);
+            if (second) swap_panels();
+            int *own_p = second ? own_pB : own_pA;
+            // rotated one column left after every step
+            for (int jj = 0; jj < nbc; ++jj) {
+                const int j = j0 + jj, buf = jj & 1;
+                unsigned long long key = 0ull;
+                int lp = 0x7fffffff, bi = 0;
+#pragma unroll
+                for (int i = 0; i < RPT; ++i) {
+                    if (row[i] < V && lpos[i] >= j) {
+                        const unsigned long long ki = (unsigned long long)__double_as_longlong(fabs(a[i][0]));
+                        if (ki > key || (ki == key && lpos[i] < lp)) {
+                            key = ki;
+                            lp = lpos[i];
+                            bi = i;
+                        }
+                    }
+                }
+                if (warp_argmax_fast(key, lp)) {
+                    double d = a[0][0];
+#pragma unroll
+                    for (int i = 1; i < RPT; ++i)
+                        if (bi == i) d = a[i][0];
+                    const double inv = (key == 0ull) ? 0.0 : recip_nr(d);
+                    ck[buf][warp] = key;
+                    cl[buf][warp] = lp;
+                    cphys[buf][warp] = tid + bi * T;
+                    cval[buf][warp] = d;
+                    crow[buf][warp][0] = inv;
+#pragma unroll
+                    for (int i = 0; i < RPT; ++i)
+                        if (bi == i) {
+#pragma unroll
+                            for (int q = 1; q < NB; ++q) crow[buf][warp][q] = a[i][q] * inv;
+                        }
+                }
+                __syncthreads();
+                unsigned long long kb = (lane < NW) ? ck[buf][lane] : 0ull;
+                int lb = (lane < NW) ? cl[buf][lane] : 0x7fffffff;
+                const bool wme = warp_argmax_fast(kb, lb) && lane < NW;
+                const int w = __ffs(__ballot_sync(0xffffffffu, wme)) - 1;
+                const int p = cphys[buf][w];
+                lb = cl[buf][w];
+                double prs[NB];
+#pragma unroll
+                for (int q = 0; q < NB; q += 2) {
+                    const double2 t2 = *reinterpret_cast<const double2 *>(&crow[buf][w][q]);
+                    prs[q] = t2.x;
+                    prs[q + 1] = t2.y;
+                }
+                if (tid == 0) {
+                    const bool singular = (ck[buf][w] == 0ull);
+                    ipiv[j] = lb;
+                    diag[j] = singular ? 0.0 : cval[buf][w];
+                    own_p[jj] = p;
+                    if (singular) atomicCAS(info, 0, j + 1);
+                }
+#pragma unroll
+                for (int i = 0; i < RPT; ++i) {
+                    if (row[i] == p) {
+#pragma unroll
+                        for (int q = 0; q < NB; ++q) a[i][q] = prs[q];
+                    } else {
+                        const double f = a[i][0];
+                        a[i][0] = -f * prs[0];
+#pragma unroll
+                        for (int q = 1; q < NB; ++q) a[i][q] = fma(-f, prs[q], a[i][q]);
+                    }
+                    if (lpos[i] == j) lpos[i] = lb;
+                    else if (lpos[i] == lb) lpos[i] = j;
+                    rotate_left(a[i]);
+                }
+            }
+            for (int e = nbc; e < NB; ++e) {
+#pragma unroll
+                for (int i = 0; i < RPT; ++i) rotate_left(a[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < RPT; ++i)
+#pragma unroll
+                for (int q = 0; q < NB; ++q)
+                    if (row[i] < V && q < nbc) panels[(size_t)(j0 + q) * V + row[i]] = a[i][q];
+            __syncthreads();
+            if (tid == 0 && k != withhold) st_release_u32(ready + k, epoch);
+            // the panel in shared memory takes this panel's update like every
+            // other CTA's; then the panels return to their places
+            if (hasB) apply_panel(k, j0, nbc, false, true);
+            if (second) swap_panels();
+        } else {
+            const int buf = k & 1;
+            if (warp == 0) {
+                int ok = 1;
+                if (lane == 0) ok = wait_ready(ready + k, epoch, (k + 1 == pA || k + 1 == pB) ? 0u : 256u);
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                __syncwarp();
+                if (ok) {
+                    if (lane < nbc) s_ip[buf][lane] = __ldcg(ipiv + j0 + lane);
+                } else if (lane == 0) {
+                    s_abort = 1;
+                    atomicExch(info + 1, 1);
+                }
+            }
+            __syncthreads();
+            if (s_abort) return;
+#pragma unroll
+            for (int i = 0; i < RPT; ++i)
+#pragma unroll
+                for (int m = 0; m < NB; ++m) {
+                    if (m < nbc) {
+                        const int j = j0 + m, ip = s_ip[buf][m];
+                        if (lpos[i] == j) lpos[i] = ip;
+                        else if (lpos[i] == ip) lpos[i] = j;
+                    }
+                }
+            apply_panel(k, j0, nbc, true, hasB);
+        }
+    }
+    __syncthreads();
+    // every panel has been seen: place the inverse, X(lpos, P_j) = Y(r, j)
+#pragma unroll
+    for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int q = 0; q < NB; ++q)
+            if (row[i] < V) {
+                if (q < ncolA) M[(size_t)own_pA[q] * V + lpos[i]] = a[i][q];
+                if (q < ncolB) M[(size_t)own_pB[q] * V + lpos[i]] = sB[q * LD + row[i]];
+            }
+    // the last panel's owner has acquired every flag: log|det| and sign
+    if (b == last_owner) {
+        double l = 0.0;
+        int neg = 0;
+        for (int i = tid; i < V; i += T) {
+            const double d = __ldcg(diag + i);
+            l += log(fabs(d));
+            if (!(d > 0)) neg ^= 1;
+            if (__ldcg(ipiv + i) != i) neg ^= 1;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            l += __shfl_down_sync(0xffffffffu, l, o);
+            neg ^= __shfl_down_sync(0xffffffffu, neg, o);
+        }
+        if (lane == 0) {
+            s_l[warp] = l;
+            s_n[warp] = neg;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            int n = 0;
+            for (int i = 0; i < NW; ++i) {
+                t += s_l[i];
+                n ^= s_n[i];
+            }
+            diag[V] = t;
+            diag[V + 1] = n ? -1.0 : 1.0;
+            sync[0] = epoch;
+        }
+    }
+}
+
 // composed column permutation: applying the interchanges last-first as column
 // swaps leaves column c of the result at column src[c] of the elimination output
 __global__ void k_compose_perm(const int *__restrict__ ipiv, int V, int *__restrict__ perm) {
@@ -708,11 +1011,39 @@ bool lu_shape_ok(int V, int rpt) {
 
 namespace {
 
+// Two panels per CTA (1024 < V <= 2304): all ceil(P/2) CTAs resident at once,
+// each with the second panel's 160 KB of shared memory.
+int run_dataflow2(double *M, LUWork &w, cudaStream_t st) {
+    const int V = w.V;
+    if (V <= 1024 || V > kLu2MaxV || w.sync == nullptr || w.sync_words < lu_sync_words(V))
+        return EPHMC_ERR_UNSUPPORTED;
+    const int P = (V + kLuPanel - 1) / kLuPanel, ncta = (P + 1) / 2;
+    int dev = 0, sms = 0, coop = 0;
+    EPHMC_CUDA(cudaGetDevice(&dev));
+    EPHMC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    EPHMC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) return EPHMC_ERR_UNSUPPORTED;
+    const size_t smem = sizeof(double) * kLuPanel * (size_t)kLu2Rows;
+    EPHMC_CUDA(cudaFuncSetAttribute(k_gj_dataflow2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    EPHMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_dataflow2, kLu2Threads, smem));
+    if ((long)per_sm * sms < ncta) return EPHMC_ERR_UNSUPPORTED;
+    double *panels = w.X;
+    int withhold = g_lu_withhold.exchange(-1);  // one call only
+    void *args[] = {&M, (void *)&V, &panels, &w.ipiv, &w.diag, &w.info, &w.sync, &withhold};
+    EPHMC_CUDA(cudaLaunchCooperativeKernel((const void *)k_gj_dataflow2, dim3(ncta), dim3(kLu2Threads), args, smem,
+                                           st));
+    ephmc::count_launch(1);
+    return EPHMC_OK;
+}
+
 // The dataflow kernel needs all ceil(V/8) CTAs resident at once; returns
-// EPHMC_ERR_UNSUPPORTED (nothing launched) when they are not, or V > 1024.
+// EPHMC_ERR_UNSUPPORTED (nothing launched) when they are not; above V = 1024
+// the two-panel kernel.
 int run_dataflow(double *M, LUWork &w, cudaStream_t st) {
     const int V = w.V;
-    if (V > 1024 || w.sync == nullptr || w.sync_words < lu_sync_words(V)) return EPHMC_ERR_UNSUPPORTED;
+    if (V > 1024) return run_dataflow2(M, w, st);
+    if (w.sync == nullptr || w.sync_words < lu_sync_words(V)) return EPHMC_ERR_UNSUPPORTED;
     const int nblk = (V + kLuPanel - 1) / kLuPanel;
     int dev = 0, sms = 0, coop = 0;
     EPHMC_CUDA(cudaGetDevice(&dev));

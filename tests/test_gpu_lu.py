@@ -26,7 +26,10 @@ def _ctx(V):
     return ephmc.Context(l1, V // l1, 1, [0.1, 0.1, 0.1], [0.0, 0.0, 0.0], -1.0, 0.1)
 
 
-def test_lu_wait_timeout_reports_and_recovers(gpu):
+@pytest.mark.parametrize("V", [256, 1600])
+def test_lu_wait_timeout_reports_and_recovers(gpu, V):
+    """V = 256: one panel per CTA; V = 1600: two panels per CTA (the second
+    in shared memory), the kernel of 1024 < V <= 2304."""
     import scipy.linalg as sl
 
     import ephmc
@@ -34,7 +37,6 @@ def test_lu_wait_timeout_reports_and_recovers(gpu):
     lib.ephmc_test_lu_withhold_next.restype = None
     lib.ephmc_test_lu_withhold_next.argtypes = [C.c_int]
     rng = np.random.default_rng(5)
-    V = 256
     with _ctx(V) as ctx:
         A = rng.standard_normal((V, V)) + 3 * np.eye(V)
         lib.ephmc_test_lu_withhold_next(3)
