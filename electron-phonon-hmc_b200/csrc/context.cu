@@ -1250,7 +1250,7 @@ int ephmc_ctx_autotune(ephmc_ctx *c, const double *x, int mode, float *ms_before
     const bool adj = mode != EPHMC_FORCE_REFERENCE && !c->flags.constant_force;
     const bool mixed = mode == EPHMC_FORCE_MIXED;
     const int Ss[5] = {1, 2, 4, 8, 16}, Rs[6] = {1, 2, 3, 4, 6, 8};
-    // k_slices: M_hat unless the strip kernel builds it; the reference force's G_t passes
+    // k_slices: M_hat unless a strip or tile kernel builds it; the reference force's G_t passes
     const bool slices_mhat = !(adj && slices_strip_supported(c->lat));
     if (slices_mhat || !adj) {
         int bS = c->lat.tune_slices_S, bR = c->lat.tune_slices_R;
@@ -1274,7 +1274,7 @@ int ephmc_ctx_autotune(ephmc_ctx *c, const double *x, int mode, float *ms_before
         c->lat.tune_slices_S = bS;
         c->lat.tune_slices_R = bR;
     }
-    // k_adjoint: the adjoint force unless the strip kernel runs it (mixed, L1 = 32)
+    // k_adjoint: the adjoint force unless a register-layout kernel runs it (mixed; L1 = 8, 12, 16, 24, 32)
     if (adj && !(mixed && adjoint_strip_supported(c->lat))) {
         float tb[3];
         if ((rc = phases(tb))) return ret(rc);

@@ -220,8 +220,10 @@ EPHMC_API int ephmc_ctx_set_segment(ephmc_ctx *ctx, unsigned length);
  * det only (one chain of QR steps). */
 EPHMC_API int ephmc_ctx_set_stabilize(ephmc_ctx *ctx, int on);
 /* No counterpart in the reference.  Chooses the launch shapes of the
- * thread-per-site sweeps (sites per thread, vectors per CTA) and the
- * dataflow LU's rows per thread for this context by timing each candidate
+ * thread-per-site sweeps (sites per thread, vectors per CTA; the strip and
+ * tile kernels of L1 = 8, 12, 16, 24, 32, 48 have fixed shapes and are not
+ * tuned) and the dataflow LU's rows per thread (V <= 1024) for this context
+ * by timing each candidate
  * over a few evaluations of x (host or device) with force_mode, and keeps
  * the fastest.  The sweeps sum in the same order for every shape (M_hat is
  * unchanged); the LU's pivots and inverse are unchanged, and its log det is
