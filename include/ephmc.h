@@ -369,7 +369,7 @@ EPHMC_API unsigned long long ephmc_launch_count(void);
 EPHMC_API int ephmc_measure_fma_peak(int fp64, float *tflops);
 
 /* No counterpart in the reference.  Test hook of the LU's failure path: the
- * next dataflow LU launch (V <= 1024) does not set the ready flag of panel
+ * next dataflow LU launch (V <= 2304) does not set the ready flag of panel
  * `panel`, so the CTAs that wait for it give up after their bounded wait (2 s)
  * and the call returns EPHMC_ERR_TIMEOUT, with the flags cleared for the next
  * call.  -1 cancels.  Affects one launch only. */
