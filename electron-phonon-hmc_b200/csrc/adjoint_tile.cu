@@ -8,8 +8,8 @@
 // L1 / W lanes of a group of LPR lanes hold a lattice row, W consecutive
 // columns per lane; a warp holds 32 / LPR groups, each a strip of H rows.  A
 // CTA has KG independent vector groups (named barriers per group); a group
-// carries VT's vectors (float: one; float2: two, as the halves of packed
-// FP32 pairs) through the slices of its segment.  Column neighbours come from
+// carries two vectors, the halves of packed FP32 pairs, through the slices
+// of its segment.  Column neighbours come from
 // the thread's registers or, at the block's edges, by warp shuffles (two per
 // row); the rows just outside a strip from shared memory.  In the link
 // contraction a thread forms, for each of its sites, the right link, the up
@@ -26,19 +26,9 @@ namespace {
 constexpr unsigned kFullA = 0xffffffffu;
 constexpr int kSlotsT = 9;  // edge rows exchanged at the widest level
 
+// packed FP32 pairs (the kernel's vector type is a template parameter; the
+// shapes in use all carry two vectors per group)
 template <typename VT> struct VOps;
-template <> struct VOps<float> {
-    static constexpr int kVec = 1;
-    static __device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-    static __device__ __forceinline__ float dup(float c) { return c; }
-    static __device__ __forceinline__ float shfl(float v, int src) { return __shfl_sync(kFullA, v, src); }
-    static __device__ __forceinline__ float sum(float v) { return v; }
-    static __device__ __forceinline__ float make(float a, float) { return a; }
-    static __device__ __forceinline__ float lo(float v) { return v; }
-    static __device__ __forceinline__ float hi(float v) { return v; }
-};
 template <> struct VOps<float2> {
     static constexpr int kVec = 2;
     static __device__ __forceinline__ float2 fma_(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }

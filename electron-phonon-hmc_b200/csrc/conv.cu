@@ -132,15 +132,6 @@ __global__ void k_conv_t_sum(const double *__restrict__ terms, int n, double h, 
     out[e] = h * sum;
 }
 
-bool conv_devp(const void *p) {
-    cudaPointerAttributes a{};
-    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
 // device copies of the inputs and the output buffer of one call
 struct ConvBufs {
     double *sigma = nullptr, *widths = nullptr, *out = nullptr, *terms = nullptr;

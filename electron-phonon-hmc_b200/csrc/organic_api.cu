@@ -216,13 +216,6 @@ struct DView {
     }
 };
 
-double host_read(const double *p) {
-    double v = 0;
-    if (devp(p)) cudaMemcpy(&v, p, sizeof(double), cudaMemcpyDeviceToHost);
-    else v = *p;
-    return v;
-}
-
 // --------------------------------------------------------------- contractions of the correlator output
 // contr_gr_mat / contr_gr_triangle / contract_greens (simulation/organic_lattice.c:62-106)
 double contract_greens_h(const double *gr, const double *mat, unsigned nn, unsigned tau) {
