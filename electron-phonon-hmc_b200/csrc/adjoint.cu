@@ -36,11 +36,14 @@ __device__ __forceinline__ Real stencil_at(const Real *__restrict__ v, int j, co
 // MODE 0: all slices from M^-1 (the range fields are not read); 1: one
 // segment of a checkpointed sweep (AdjointRange t0, t1, q_top, y_in, y_out);
 // 2: the segment grid (AdjointRange seg_*), one segment per blockIdx.y
-// WIDE: at most 320 threads, so that S = 8 sites keep their tables in 168
-// registers instead of spilling (the FP32 force at 48x48, Nt = 128: 27.2 ms
-// instead of 39.5)
+// WIDE: one CTA per SM of at most 320 threads for S = 8, so that eight
+// sites keep their tables in 168 registers instead of spilling (the FP32
+// force at 48x48, Nt = 128: 27.2 ms instead of 39.5), or of at most 640
+// threads for S = 4: the FP32 sweep's four sites fit in 96 registers, and
+// at 48x48 18 warps per SM instead of 9 hide more of the stencils' latency
+// (force phase 38.5 -> 33.9 ms)
 template <typename Real, typename QT, int S, int MODE, bool WIDE = false>
-__global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
+__global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
                           const int *__restrict__ ev_fac, const int *__restrict__ nbr,
                           const QT *__restrict__ qstack, const double *__restrict__ Minv, int V, int nt,
                           int R, double pref_scale, double *__restrict__ force, AdjointRange rg_in) {
@@ -74,14 +77,33 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *_
     const Real al0 = (Real)c.a_lin[0], aq0 = (Real)c.a_quad[0];
     const Real al1 = (Real)c.a_lin[1], aq1 = (Real)c.a_quad[1];
 
-    int src[S][6], nb[S][3];
+    // A site's three forward neighbours are consecutive in its event list
+    // (its own links sort as one block between the incoming ones): nbr[k][j]
+    // = src[p + k] with p in 0..3.  The FP32 sweep keeps two bits per site in
+    // pos instead of three registers per site (at 48x48 it then spills
+    // nothing); the FP64 sweep, which spills more that way, keeps nb.  On
+    // lattices small enough for one site to appear twice, any p whose three
+    // entries match gives the same neighbours.
+    constexpr bool kPack = sizeof(Real) == 4;
+    int src[S][6], nb[kPack ? 1 : S][3];
+    unsigned pos = 0;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         const int j = tid + s * T;
 #pragma unroll
         for (int e = 0; e < 6; ++e) src[s][e] = (j < V) ? ev_src[e * V + j] : 0;
+        const int n0 = (j < V) ? nbr[j] : 0, n1 = (j < V) ? nbr[V + j] : 0, n2 = (j < V) ? nbr[2 * V + j] : 0;
+        if (kPack) {
+            unsigned p = 3;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) nb[s][k] = (j < V) ? nbr[k * V + j] : 0;
+            for (int q = 2; q >= 0; --q)
+                if (src[s][q] == n0 && src[s][q + 1] == n1 && src[s][q + 2] == n2) p = (unsigned)q;
+            pos |= p << (2 * s);
+        } else {
+            nb[kPack ? 0 : s][0] = n0;
+            nb[kPack ? 0 : s][1] = n1;
+            nb[kPack ? 0 : s][2] = n2;
+        }
     }
 
     // y(t0): row c of M^-1 (math) = column c of the inverse's array, the rows
@@ -184,7 +206,12 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *_
                     const Real L3i = fma(al1, F0Q[i], aq1 * HF0Q[i]);
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
-                        const int n = nb[s][k];
+                        const unsigned p = (pos >> (2 * s)) & 3u;
+                        const int n = !kPack  ? nb[kPack ? 0 : s][k]
+                                      : p == 0 ? src[s][k]
+                                      : p == 1 ? src[s][k + 1]
+                                      : p == 2 ? src[s][k + 2]
+                                               : src[s][k + 3];
                         const Real L1n = fma(al0, Q[n], aq0 * HQ[n]);
                         const Real L3n = fma(al1, F0Q[n], aq1 * HF0Q[n]);
                         Real d = L1i * F1Y[n];
@@ -218,6 +245,20 @@ __global__ void __launch_bounds__(WIDE ? 320 : 512, 1) k_adjoint(const double *_
     }
 }
 
+template <typename Real, typename QT>
+using AdjointKernel = void (*)(const double *, Couplings, const int *, const int *, const int *, const QT *,
+                               const double *, int, int, int, double, double *, AdjointRange);
+
+// the instance of a mode; the FP64 sweep has none at 640 threads
+template <typename Real, typename QT, int S, bool WIDE = false>
+AdjointKernel<Real, QT> pick_adjoint(int mode) {
+    if constexpr (WIDE && S == 4 && sizeof(Real) == 8)
+        return pick_adjoint<Real, QT, S, false>(mode);
+    else
+        return mode == 2 ? k_adjoint<Real, QT, S, 2, WIDE>
+                         : mode == 1 ? k_adjoint<Real, QT, S, 1, WIDE> : k_adjoint<Real, QT, S, 0, WIDE>;
+}
+
 }  // namespace
 
 template <typename Real, typename QT>
@@ -226,8 +267,10 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
                          double *force, cudaStream_t st, const AdjointRange *range, int seg_count) {
     const int V = lat.V;
     int S = 16;
+    // the fewest sites per thread within the thread limit: 512, or 640 for
+    // the FP32 sweep at four sites (the FP64 one spills there)
     for (int o : {1, 2, 4, 8, 16})
-        if ((V + o - 1) / o <= 512) { S = o; break; }
+        if ((V + o - 1) / o <= adjoint_max_threads(o, sizeof(Real) == 4)) { S = o; break; }
     int T = (((V + S - 1) / S) + 31) / 32 * 32;
     const size_t per_vec = 9 * (size_t)V * sizeof(Real);
     const size_t fac_b = 3 * (size_t)V * sizeof(Real);
@@ -244,7 +287,8 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     // a tuned shape (ephmc_ctx_autotune) replaces the rule when it is valid
     {
         const int tS = lat.tune_adj_S, tR = lat.tune_adj_R;
-        if ((tS == 1 || tS == 2 || tS == 4 || tS == 8 || tS == 16) && (V + tS - 1) / tS <= 512) {
+        if ((tS == 1 || tS == 2 || tS == 4 || tS == 8 || tS == 16) &&
+            (V + tS - 1) / tS <= adjoint_max_threads(tS, sizeof(Real) == 4)) {
             S = tS;
             T = (((V + S - 1) / S) + 31) / 32 * 32;
         }
@@ -256,23 +300,15 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     AdjointRange rg{0, nt, nullptr, nullptr, nullptr, true};
     if (range) rg = *range;
     if (rg.zero_force) EPHMC_CUDA(cudaMemsetAsync(force, 0, sizeof(double) * (size_t)nt * V * 3, st));
-    void (*kern)(const double *, Couplings, const int *, const int *, const int *, const QT *, const double *,
-                 int, int, int, double, double *, AdjointRange) = nullptr;
     const int mode = rg.seg_C > 0 ? 2 : range != nullptr ? 1 : 0;
-#define EPHMC_ADJ_PICK(SS, ...)                                                              \
-    (mode == 2 ? k_adjoint<Real, QT, SS, 2, ##__VA_ARGS__>                                  \
-               : mode == 1 ? k_adjoint<Real, QT, SS, 1, ##__VA_ARGS__> : k_adjoint<Real, QT, SS, 0, ##__VA_ARGS__>)
+    AdjointKernel<Real, QT> kern = nullptr;
     switch (S) {
-        case 1: kern = EPHMC_ADJ_PICK(1); break;
-        case 2: kern = EPHMC_ADJ_PICK(2); break;
-        case 4: kern = EPHMC_ADJ_PICK(4); break;
-        case 8:
-            if (T <= 320) kern = EPHMC_ADJ_PICK(8, true);
-            else kern = EPHMC_ADJ_PICK(8);
-            break;
-        default: kern = EPHMC_ADJ_PICK(16); break;
+        case 1: kern = pick_adjoint<Real, QT, 1>(mode); break;
+        case 2: kern = pick_adjoint<Real, QT, 2>(mode); break;
+        case 4: kern = T > 512 ? pick_adjoint<Real, QT, 4, true>(mode) : pick_adjoint<Real, QT, 4>(mode); break;
+        case 8: kern = T <= 320 ? pick_adjoint<Real, QT, 8, true>(mode) : pick_adjoint<Real, QT, 8>(mode); break;
+        default: kern = pick_adjoint<Real, QT, 16>(mode); break;
     }
-#undef EPHMC_ADJ_PICK
     EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const dim3 grid((V + R - 1) / R, mode == 2 ? (unsigned)seg_count : 1u);
     kern<<<grid, T, smem, st>>>(x, c, lat.ev_src, lat.ev_fac, lat.nbr, qstack, Minv, V, nt, R, pref, force, rg);

@@ -1282,7 +1282,7 @@ int ephmc_ctx_autotune(ephmc_ctx *c, const double *x, int mode, float *ms_before
         float best = tb[2];
         const size_t real = mixed ? sizeof(float) : sizeof(double);
         for (int S : Ss) {
-            if ((V + S - 1) / S > 512) continue;
+            if ((V + S - 1) / S > adjoint_max_threads(S, mixed)) continue;
             for (int R = 1; R <= 4; ++R) {
                 if (3 * (size_t)V * real + 9 * (size_t)V * real * R > 200 * 1024) continue;
                 c->lat.tune_adj_S = S;

@@ -204,7 +204,9 @@ int launch_link_refine(const double *x, const Couplings &c, const LatticeDev &la
                        cudaStream_t st);
 
 // Adjoint sweep 2 (see adjoint.cu): y chain forward from M^-1, contraction with
-// the stored q(t).
+// the stored q(t).  One thread per S sites, at most adjoint_max_threads(S)
+// threads per CTA (the launch bounds of its instances).
+inline int adjoint_max_threads(int S, bool fp32) { return S == 4 && fp32 ? 640 : 512; }
 template <typename Real, typename QT>
 int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat,
                          const QT *qstack, const double *Minv, int nt, unsigned flavors,

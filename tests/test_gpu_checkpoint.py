@@ -46,7 +46,7 @@ def test_checkpointed_force_equals_whole_stack(gpu, restated, shape, mode):
         assert ld == ld0 and _rel(pd, pd0) <= tol
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 64, 20.0), (12, 12, 37, 10.0)])
+@pytest.mark.parametrize("shape", [(32, 32, 64, 20.0), (12, 12, 37, 10.0), (10, 10, 23, 8.0)])
 def test_checkpointed_mixed_force_equals_segmented_whole_stack(gpu, restated, shape):
     """The mixed force's segments are the checkpoint interval: checkpointed
     (one FP32 region reused, segments bottom up, y chain in place) against
@@ -57,7 +57,8 @@ def test_checkpointed_mixed_force_equals_segmented_whole_stack(gpu, restated, sh
     the FP32 sweep: the forces agree to 1e-6, and with segments of at most 16
     slices each is within 1e-5 of the FP64 force.  C >= Nt is one segment,
     the unsegmented FP32 sweep, whose error against FP64 (2e-3 at 32x32,
-    Nt = 64) is what segmenting removes."""
+    Nt = 64) is what segmenting removes.  10x10 runs the shared-memory
+    sweep (no register-strip or tile shape) segment by segment."""
     import ephmc
     from oracle import Model
     l1, l2, nt, beta = shape
@@ -65,7 +66,7 @@ def test_checkpointed_mixed_force_equals_segmented_whole_stack(gpu, restated, sh
     x = restated.random_x(3, m.dim)
     with ephmc.Context(m.l1, m.l2, m.nt, m.t, m.kappa, m.mu, m.omega) as ctx:
         ld64, pd64 = ctx.eval(x, mode="adjoint")
-        for C in (1, 8, 12, nt, nt + 5):
+        for C in (1, 8, 12, nt, nt + 5) if l1 != 10 else (1, 2, 3, 8, nt):
             ctx.set_checkpoint(0)
             ctx.set_segment(C)
             ld_w, pd_w = ctx.eval(x, mode="mixed")
@@ -103,7 +104,7 @@ def test_checkpointed_single_particle_and_device_buffers(gpu, restated):
 def test_cfg2_checkpoint_memory(gpu, restated):
     """48x48 (V = 2304), Nt = 128, beta = 40, checkpoints every 12 slices:
     10 FP64 checkpoints + a 12-slice segment (0.93 GB) instead of the
-    5.4 GB stack; the context goes from 5.7 GB to 1.2 GB (measured 1.22);
+    5.4 GB stack; the context goes from 7.1 GB to 1.3 GB (measured 1.26);
     mixed force as with the whole stack."""
     import ephmc
     from oracle import Model
