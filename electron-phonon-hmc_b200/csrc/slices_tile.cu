@@ -45,6 +45,25 @@ __device__ __forceinline__ Real stencil_t(const HopT<Real> &h, Real mu, Real v, 
 
 template <typename T, typename Real> __device__ __forceinline__ void st_t(T *p, Real v) { *p = (T)v; }
 
+// The hopping field of one slice (3V doubles) into shared memory by
+// asynchronous copies spread over the CTA: 16 bytes per copy when x and the
+// slice size allow it, else 8.  The caller commits the group and waits for it
+// with cp.async.wait_group (a hardware wait; no copy is left in flight at exit).
+__device__ __forceinline__ void stage_field(double *dst, const double *src, int n3, bool vec16) {
+    if (vec16) {
+        for (int e = 2 * (int)threadIdx.x; e < n3; e += 2 * (int)blockDim.x)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst + e)),
+                         "l"(src + e)
+                         : "memory");
+    } else {
+        for (int e = (int)threadIdx.x; e < n3; e += (int)blockDim.x)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst + e)),
+                         "l"(src + e)
+                         : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
 // Thread geometry of the tile layout
 struct Tile {
     int L1, L2, NS;  // lattice extents, strips
@@ -120,6 +139,9 @@ __device__ __forceinline__ void apply_H_tile(const Real (&v)[R][H][W], Real (&w)
     __syncthreads();  // the edge buffer is reused by the next stencil
 }
 
+// byte offset of the staged hopping fields after the edge rows
+__host__ __device__ constexpr size_t tile_field_offset(size_t edge_bytes) { return (edge_bytes + 15) / 16 * 16; }
+
 // Real: the arithmetic (double; float for stacks that start from the
 // identity and only feed the mixed force, as in the L1 = 32 FP32 kernel)
 template <typename Real, typename StackT, int R, int H, int W, int LPR, int MAXT>
@@ -130,6 +152,11 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
     const SliceJob job = jobs[blockIdx.y];
     const Tile t = tile_of<W, LPR, H>(L1, L2);
     const int V = L1 * L2;
+    // the slices' hopping fields, [2][3V] doubles after the edge rows (16-byte
+    // aligned): slice it + 1 is copied while slice it is computed
+    const int n3 = 3 * V;
+    double *xbuf = reinterpret_cast<double *>(smem_t + tile_field_offset(sizeof(Real) * 2 * R * (size_t)t.NS * L1));
+    const bool vec16 = (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (n3 & 1) == 0;
     const size_t VV = (size_t)V * V;
     const int vec0 = blockIdx.x * R;
     const Real mu = (Real)cp.mu;
@@ -148,9 +175,14 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
             }
     }
     const int bd = t.b0 == 0 ? L2 - 1 : t.b0 - 1;  // the row below the strip
+    if (job.s_count > 0) stage_field(xbuf, x + (size_t)job.s_first * n3, n3, vec16);
     for (int it = 0; it < job.s_count; ++it) {
         const int sl = job.s_first + it * job.s_dir;
-        const double *xs = x + (size_t)sl * 3 * V;
+        asm volatile("cp.async.wait_group 0;" ::: "memory");  // this thread's copies of slice it
+        __syncthreads();  // everyone's, and every thread is past slice it - 1 (its buffer is free)
+        if (it + 1 < job.s_count)
+            stage_field(xbuf + (size_t)((it + 1) & 1) * n3, x + (size_t)(sl + job.s_dir) * n3, n3, vec16);
+        const double *xs = xbuf + (size_t)(it & 1) * n3;
         // hopping coefficients of the thread's sites (its own links), and of
         // the neighbours they take from (left: link 0, below: link 1, below
         // right: link 2) from its registers, the neighbouring lanes, or, for
@@ -161,9 +193,9 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
 #pragma unroll
             for (int k = 0; k < W; ++k) {
                 const double *xi = xs + 3 * ((t.b0 + h) * L1 + t.a0 + k);
-                hp[h][k].f0 = (Real)fma(-cp.kappa[0], __ldg(xi + 0), cp.t[0]);
-                hp[h][k].f1 = (Real)fma(-cp.kappa[1], __ldg(xi + 1), cp.t[1]);
-                hp[h][k].f2 = (Real)fma(-cp.kappa[2], __ldg(xi + 2), cp.t[2]);
+                hp[h][k].f0 = (Real)fma(-cp.kappa[0], xi[0], cp.t[0]);
+                hp[h][k].f1 = (Real)fma(-cp.kappa[1], xi[1], cp.t[1]);
+                hp[h][k].f2 = (Real)fma(-cp.kappa[2], xi[2], cp.t[2]);
             }
 #pragma unroll
         for (int h = 0; h < H; ++h) {
@@ -183,8 +215,8 @@ __global__ void __launch_bounds__(MAXT) k_slices_tile(const double *__restrict__
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const int a = t.a0 + k, ar = a + 1 == L1 ? 0 : a + 1;
-            hp[0][k].f1d = (Real)fma(-cp.kappa[1], __ldg(xs + 3 * (bd * L1 + a) + 1), cp.t[1]);
-            hp[0][k].f2dr = (Real)fma(-cp.kappa[2], __ldg(xs + 3 * (bd * L1 + ar) + 2), cp.t[2]);
+            hp[0][k].f1d = (Real)fma(-cp.kappa[1], xs[3 * (bd * L1 + a) + 1], cp.t[1]);
+            hp[0][k].f2dr = (Real)fma(-cp.kappa[2], xs[3 * (bd * L1 + ar) + 2], cp.t[2]);
         }
         for (int p = job.p_begin; p != job.p_end; p += job.p_step) {
             // p is 0 or 1; selecting avoids indexing the parameter struct at run time
@@ -267,10 +299,14 @@ int launch_tile(const double *x, const Couplings &c, const LatticeDev &lat, cons
     const int V = lat.V, L1 = lat.l1, L2 = lat.l2, NS = L2 / H;
     const int threads = 32 * NS / G;
     if (threads > MAXT) return EPHMC_ERR_UNSUPPORTED;
-    const size_t smem = sizeof(Real) * 2 * R * (size_t)NS * L1;
-    if (smem > 48 * 1024) return EPHMC_ERR_UNSUPPORTED;
+    const size_t edge = sizeof(Real) * 2 * R * (size_t)NS * L1;
+    if (edge > 48 * 1024) return EPHMC_ERR_UNSUPPORTED;
+    const size_t smem = tile_field_offset(edge) + 2 * 3 * sizeof(double) * (size_t)V;  // + two slices' fields
+    if (smem > 227 * 1024) return EPHMC_ERR_UNSUPPORTED;
+    auto kern = k_slices_tile<Real, StackT, R, H, W, LPR, MAXT>;
+    EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((V + R - 1) / R, njobs);
-    k_slices_tile<Real, StackT, R, H, W, LPR, MAXT><<<grid, threads, smem, st>>>(x, c, jobs, L1, L2);
+    kern<<<grid, threads, smem, st>>>(x, c, jobs, L1, L2);
     ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());
     return EPHMC_OK;
