@@ -42,7 +42,7 @@ __device__ __forceinline__ Real stencil_at(const Real *__restrict__ v, int j, co
 // threads for S = 4: the FP32 sweep's four sites fit in 96 registers, and
 // at 48x48 18 warps per SM instead of 9 hide more of the stencils' latency
 // (force phase 38.5 -> 33.9 ms)
-template <typename Real, typename QT, int S, int MODE, bool WIDE = false>
+template <typename Real, typename QT, int S, int MODE, bool WIDE, bool PACK>
 __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoint(const double *__restrict__ x, Couplings c, const int *__restrict__ ev_src,
                           const int *__restrict__ ev_fac, const int *__restrict__ nbr,
                           const QT *__restrict__ qstack, const double *__restrict__ Minv, int V, int nt,
@@ -77,14 +77,16 @@ __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoin
     const Real al0 = (Real)c.a_lin[0], aq0 = (Real)c.a_quad[0];
     const Real al1 = (Real)c.a_lin[1], aq1 = (Real)c.a_quad[1];
 
-    // A site's three forward neighbours are consecutive in its event list
-    // (its own links sort as one block between the incoming ones): nbr[k][j]
-    // = src[p + k] with p in 0..3.  The FP32 sweep keeps two bits per site in
-    // pos instead of three registers per site (at 48x48 it then spills
-    // nothing); the FP64 sweep, which spills more that way, keeps nb.  On
+    // A site's three forward neighbours are, on most lattices, consecutive in
+    // its event list (its own links sort as one block between the incoming
+    // ones): nbr[k][j] = src[p + k] with p in 0..3.  PACK (the FP32 sweep on
+    // a lattice where this holds for every site, LatticeDev::nb_in_events)
+    // keeps two bits per site in pos instead of three registers per site (at
+    // 48x48 it then spills nothing); the FP64 sweep, which spills more that
+    // way, and the lattices where a self-link breaks the block keep nb.  On
     // lattices small enough for one site to appear twice, any p whose three
     // entries match gives the same neighbours.
-    constexpr bool kPack = sizeof(Real) == 4;
+    constexpr bool kPack = PACK;
     int src[S][6], nb[kPack ? 1 : S][3];
     unsigned pos = 0;
 #pragma unroll
@@ -249,14 +251,22 @@ template <typename Real, typename QT>
 using AdjointKernel = void (*)(const double *, Couplings, const int *, const int *, const int *, const QT *,
                                const double *, int, int, int, double, double *, AdjointRange);
 
-// the instance of a mode; the FP64 sweep has none at 640 threads
+// the instance of a mode; packed neighbours only in the FP32 sweep, and no
+// unpacked instance at 640 threads
 template <typename Real, typename QT, int S, bool WIDE = false>
-AdjointKernel<Real, QT> pick_adjoint(int mode) {
-    if constexpr (WIDE && S == 4 && sizeof(Real) == 8)
-        return pick_adjoint<Real, QT, S, false>(mode);
+AdjointKernel<Real, QT> pick_adjoint(int mode, bool packed) {
+    if constexpr (sizeof(Real) == 4) {
+        if (packed)
+            return mode == 2   ? k_adjoint<Real, QT, S, 2, WIDE, true>
+                   : mode == 1 ? k_adjoint<Real, QT, S, 1, WIDE, true>
+                               : k_adjoint<Real, QT, S, 0, WIDE, true>;
+    }
+    if constexpr (WIDE && S == 4)
+        return pick_adjoint<Real, QT, S, false>(mode, false);
     else
-        return mode == 2 ? k_adjoint<Real, QT, S, 2, WIDE>
-                         : mode == 1 ? k_adjoint<Real, QT, S, 1, WIDE> : k_adjoint<Real, QT, S, 0, WIDE>;
+        return mode == 2   ? k_adjoint<Real, QT, S, 2, WIDE, false>
+               : mode == 1 ? k_adjoint<Real, QT, S, 1, WIDE, false>
+                           : k_adjoint<Real, QT, S, 0, WIDE, false>;
 }
 
 }  // namespace
@@ -266,11 +276,12 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
                          double *force, cudaStream_t st, const AdjointRange *range, int seg_count) {
     const int V = lat.V;
+    const bool packed = sizeof(Real) == 4 && lat.nb_in_events;
     int S = 16;
     // the fewest sites per thread within the thread limit: 512, or 640 for
-    // the FP32 sweep at four sites (the FP64 one spills there)
+    // the packed FP32 sweep at four sites (the FP64 one spills there)
     for (int o : {1, 2, 4, 8, 16})
-        if ((V + o - 1) / o <= adjoint_max_threads(o, sizeof(Real) == 4)) { S = o; break; }
+        if ((V + o - 1) / o <= adjoint_max_threads(o, packed)) { S = o; break; }
     int T = (((V + S - 1) / S) + 31) / 32 * 32;
     const size_t per_vec = 9 * (size_t)V * sizeof(Real);
     const size_t fac_b = 3 * (size_t)V * sizeof(Real);
@@ -288,7 +299,7 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     {
         const int tS = lat.tune_adj_S, tR = lat.tune_adj_R;
         if ((tS == 1 || tS == 2 || tS == 4 || tS == 8 || tS == 16) &&
-            (V + tS - 1) / tS <= adjoint_max_threads(tS, sizeof(Real) == 4)) {
+            (V + tS - 1) / tS <= adjoint_max_threads(tS, packed)) {
             S = tS;
             T = (((V + S - 1) / S) + 31) / 32 * 32;
         }
@@ -303,11 +314,15 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     const int mode = rg.seg_C > 0 ? 2 : range != nullptr ? 1 : 0;
     AdjointKernel<Real, QT> kern = nullptr;
     switch (S) {
-        case 1: kern = pick_adjoint<Real, QT, 1>(mode); break;
-        case 2: kern = pick_adjoint<Real, QT, 2>(mode); break;
-        case 4: kern = T > 512 ? pick_adjoint<Real, QT, 4, true>(mode) : pick_adjoint<Real, QT, 4>(mode); break;
-        case 8: kern = T <= 320 ? pick_adjoint<Real, QT, 8, true>(mode) : pick_adjoint<Real, QT, 8>(mode); break;
-        default: kern = pick_adjoint<Real, QT, 16>(mode); break;
+        case 1: kern = pick_adjoint<Real, QT, 1>(mode, packed); break;
+        case 2: kern = pick_adjoint<Real, QT, 2>(mode, packed); break;
+        case 4:
+            kern = T > 512 ? pick_adjoint<Real, QT, 4, true>(mode, packed) : pick_adjoint<Real, QT, 4>(mode, packed);
+            break;
+        case 8:
+            kern = T <= 320 ? pick_adjoint<Real, QT, 8, true>(mode, packed) : pick_adjoint<Real, QT, 8>(mode, packed);
+            break;
+        default: kern = pick_adjoint<Real, QT, 16>(mode, packed); break;
     }
     EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const dim3 grid((V + R - 1) / R, mode == 2 ? (unsigned)seg_count : 1u);

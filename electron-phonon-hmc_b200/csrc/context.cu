@@ -121,6 +121,21 @@ int build_event_tables(const unsigned *nnt, int V, std::vector<int> &ev_src, std
     return EPHMC_OK;
 }
 
+// Whether every site's forward neighbours nbr[k][j] are three consecutive
+// entries of its event sources ev_src[e][j], e = p..p + 2 for some p in 0..3.
+bool neighbours_in_events(const std::vector<int> &ev_src, const std::vector<int> &nbr, int V) {
+    for (int j = 0; j < V; ++j) {
+        bool found = false;
+        for (int p = 0; p <= 3 && !found; ++p) {
+            found = true;
+            for (int k = 0; k < 3; ++k)
+                found = found && ev_src[(size_t)(p + k) * V + j] == nbr[(size_t)k * V + j];
+        }
+        if (!found) return false;
+    }
+    return true;
+}
+
 }  // namespace ephmc
 
 using namespace ephmc;
@@ -1129,6 +1144,7 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     cudaMemcpy(c->lat.ev_src, es.data(), sizeof(int) * 6 * V, cudaMemcpyHostToDevice);
     cudaMemcpy(c->lat.ev_fac, ef.data(), sizeof(int) * 6 * V, cudaMemcpyHostToDevice);
     cudaMemcpy(c->lat.nbr, nb.data(), sizeof(int) * 3 * V, cudaMemcpyHostToDevice);
+    c->lat.nb_in_events = neighbours_in_events(es, nb, (int)V);
     {
         std::vector<int> rv(3 * (size_t)V, 0);
         for (unsigned k = 0; k < 3; ++k)
@@ -1282,7 +1298,7 @@ int ephmc_ctx_autotune(ephmc_ctx *c, const double *x, int mode, float *ms_before
         float best = tb[2];
         const size_t real = mixed ? sizeof(float) : sizeof(double);
         for (int S : Ss) {
-            if ((V + S - 1) / S > adjoint_max_threads(S, mixed)) continue;
+            if ((V + S - 1) / S > adjoint_max_threads(S, mixed && c->lat.nb_in_events)) continue;
             for (int R = 1; R <= 4; ++R) {
                 if (3 * (size_t)V * real + 9 * (size_t)V * real * R > 200 * 1024) continue;
                 c->lat.tune_adj_S = S;

@@ -58,12 +58,19 @@ struct LatticeDev {
     // launch shapes chosen by ephmc_ctx_autotune (0: the built-in rule):
     // sites per thread and vectors per CTA of k_slices and of k_adjoint
     int tune_slices_S = 0, tune_slices_R = 0, tune_adj_S = 0, tune_adj_R = 0;
+    // every site's forward neighbours nbr[k][j] are three consecutive entries
+    // of its event sources (true unless a self-link sorts inside the site's
+    // own block, as on lattices of one row): the FP32 force sweep then keeps
+    // only their offset (adjoint.cu)
+    bool nb_in_events = false;
 };
 
 // Host helper: build the event tables; returns EPHMC_OK or EPHMC_ERR_LATTICE.
 int build_event_tables(const unsigned *nnt, int V, std::vector<int> &ev_src,
                        std::vector<int> &ev_fac, std::vector<int> &nbr);
 void triangular_lattice(unsigned l1, unsigned l2, unsigned *nnt);
+// LatticeDev::nb_in_events of the tables build_event_tables made
+bool neighbours_in_events(const std::vector<int> &ev_src, const std::vector<int> &nbr, int V);
 
 // what a captured trajectory (ephmc_leapfrog_graph) depends on besides the
 // context's buffers: field pointers, steps, length, force mode and the
@@ -205,8 +212,9 @@ int launch_link_refine(const double *x, const Couplings &c, const LatticeDev &la
 
 // Adjoint sweep 2 (see adjoint.cu): y chain forward from M^-1, contraction with
 // the stored q(t).  One thread per S sites, at most adjoint_max_threads(S)
-// threads per CTA (the launch bounds of its instances).
-inline int adjoint_max_threads(int S, bool fp32) { return S == 4 && fp32 ? 640 : 512; }
+// threads per CTA (the launch bounds of its instances; packed: the FP32
+// sweep on a lattice with nb_in_events).
+inline int adjoint_max_threads(int S, bool packed) { return S == 4 && packed ? 640 : 512; }
 template <typename Real, typename QT>
 int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &lat,
                          const QT *qstack, const double *Minv, int nt, unsigned flavors,

@@ -121,6 +121,29 @@ def test_lu_against_numpy(gpu):
             assert np.array_equal(ipiv - 1, piv)
 
 
+@pytest.mark.parametrize("shape", [(6, 1, 8), (5, 1, 12), (1, 6, 8)])
+def test_chain_lattice_forces_agree(gpu, restated, shape):
+    """Lattices of one row (L2 = 1) make every site its own upper neighbour:
+    the incoming copy of that link sorts inside the site's own event block,
+    so the FP32 shared-memory force sweep keeps its neighbour table there
+    instead of the packed offsets (one column, L1 = 1, still packs).  The
+    FP64 adjoint and the mixed force against the reference algorithm on the
+    GPU (itself pinned to the reference's fixtures above)."""
+    import ephmc
+    from oracle import Model
+    l1, l2, nt = shape
+    m = Model.physical(l1, l2, nt, 2.0)
+    x = restated.random_x(7, m.dim)
+    with ephmc.Context(m.l1, m.l2, m.nt, m.t, m.kappa, m.mu, m.omega) as ctx:
+        ld_r, pd_r = ctx.eval(x, mode="reference")
+        ld_a, pd_a = ctx.eval(x, mode="adjoint")
+        ld_m, pd_m = ctx.eval(x, mode="mixed")
+    scale = float(np.max(np.abs(pd_r)))
+    assert abs(ld_a - ld_r) <= 1e-12 * max(1.0, abs(ld_r)) and abs(ld_m - ld_a) <= 1e-12 * max(1.0, abs(ld_a))
+    assert float(np.max(np.abs(pd_a - pd_r))) <= 1e-10 * scale
+    assert float(np.max(np.abs(pd_m - pd_r))) <= 1e-5 * scale
+
+
 @pytest.mark.parametrize("kind", ["permutation", "ones_plus_identity", "small_integers", "ones_minus_identity"])
 def test_lu_ties_follow_lapack(gpu, kind):
     """Structured matrices: the pivot rows are dgetrf's, so ipiv equals
