@@ -18,6 +18,8 @@
 // One CTA owns R vectors c and walks t = 0..Nt-1, keeping all nine working
 // vectors in shared memory; partial link sums of its R vectors are added to
 // the force with one FP64 atomic per (t, site, link).
+#include <algorithm>
+
 #include "ephmc_internal.cuh"
 
 namespace ephmc {
@@ -49,6 +51,7 @@ __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoin
                           int R, double pref_scale, double *__restrict__ force, AdjointRange rg_in) {
     AdjointRange rg = rg_in;
     if (MODE == 0) rg = AdjointRange{0, nt, nullptr, nullptr, nullptr, true};
+    const float *__restrict__ lat_coef = rg_in.coef;  // packed sweep: [nt][6][V]
     // the segment of the grid (MODE 2): slices [t0, t1), identity q at t1 - 1
     int q_id_slice = nt - 1;
     if (MODE == 2) {
@@ -125,10 +128,25 @@ __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoin
 
     for (int t = rg.t0; t < rg.t1; ++t) {
         __syncthreads();
-        const double *xs = x + (size_t)t * 3 * V;
-        for (int e = tid; e < 3 * V; e += T) {
-            const int k = e % 3;
-            fac[e] = (Real)fma(-c.kappa[k], xs[e], c.t[k]);
+        // the sites' stencil coefficients: the packed sweep loads them from the
+        // slice's coefficient table (coalesced, before the barrier below); the
+        // others form the slice's link coefficients in fac and gather them
+        // through ev_fac after it
+        Real fl[S][6];
+        if (kPack) {
+            const float *cf = lat_coef + (size_t)t * 6 * V;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const int j = tid + s * T;
+#pragma unroll
+                for (int e = 0; e < 6; ++e) fl[s][e] = (j < V) ? (Real)__ldg(cf + (size_t)e * V + j) : (Real)0;
+            }
+        } else {
+            const double *xs = x + (size_t)t * 3 * V;
+            for (int e = tid; e < 3 * V; e += T) {
+                const int k = e % 3;
+                fac[e] = (Real)fma(-c.kappa[k], xs[e], c.t[k]);
+            }
         }
         if (t == q_id_slice) {
             for (int f = tid; f < nvec * V; f += T) {
@@ -144,12 +162,13 @@ __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoin
             for (int f = tid; f < nvec * V; f += T) q[f] = (Real)qs[f];
         }
         __syncthreads();
-        Real fl[S][6];
+        if (!kPack) {
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const int j = tid + s * T;
+            for (int s = 0; s < S; ++s) {
+                const int j = tid + s * T;
 #pragma unroll
-            for (int e = 0; e < 6; ++e) fl[s][e] = (j < V) ? fac[ev_fac[e * V + j]] : (Real)0;
+                for (int e = 0; e < 6; ++e) fl[s][e] = (j < V) ? fac[ev_fac[e * V + j]] : (Real)0;
+            }
         }
         // A: hq = H q, hy = H y
         for (int r = 0; r < nvec; ++r) {
@@ -247,6 +266,24 @@ __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoin
     }
 }
 
+// The packed sweep's coefficient table for slices [t0, t1): coef[t][e][j] =
+// (float)(t_k - kappa_k x[t][f]), f = ev_fac[e][j], k = f % 3 -- the value the
+// unpacked sweep forms in fac[f] and gathers through ev_fac, bit for bit.
+__global__ void __launch_bounds__(256) k_adjoint_coef(const double *__restrict__ x, Couplings c,
+                                                      const int *__restrict__ ev_fac, int V, int t0, int t1,
+                                                      float *__restrict__ coef) {
+    const size_t n6 = 6 * (size_t)V, total = (size_t)(t1 - t0) * n6;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int t = t0 + (int)(idx / n6);
+        const int r = (int)(idx % n6);  // e V + j
+        const int f = ev_fac[r], k = f % 3;
+        const double kap = k == 0 ? c.kappa[0] : k == 1 ? c.kappa[1] : c.kappa[2];
+        const double tk = k == 0 ? c.t[0] : k == 1 ? c.t[1] : c.t[2];
+        coef[(size_t)t * n6 + r] = (float)fma(-kap, x[(size_t)t * 3 * V + f], tk);
+    }
+}
+
 template <typename Real, typename QT>
 using AdjointKernel = void (*)(const double *, Couplings, const int *, const int *, const int *, const QT *,
                                const double *, int, int, int, double, double *, AdjointRange);
@@ -276,7 +313,7 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
                          const double *Minv, int nt, unsigned flavors, int single_particle, double logdet,
                          double *force, cudaStream_t st, const AdjointRange *range, int seg_count) {
     const int V = lat.V;
-    const bool packed = sizeof(Real) == 4 && lat.nb_in_events;
+    const bool packed = sizeof(Real) == 4 && lat.nb_in_events && lat.coef != nullptr && lat.coef_nt >= nt;
     int S = 16;
     // the fewest sites per thread within the thread limit: 512, or 640 for
     // the packed FP32 sweep at four sites (the FP64 one spills there)
@@ -326,6 +363,24 @@ int launch_adjoint_sweep(const double *x, const Couplings &c, const LatticeDev &
     }
     EPHMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const dim3 grid((V + R - 1) / R, mode == 2 ? (unsigned)seg_count : 1u);
+    if (packed) {  // the coefficient table of the slices this launch covers
+        int ta = 0, tb = nt;
+        if (mode == 1) {
+            ta = rg.t0;
+            tb = rg.t1;
+        } else if (mode == 2) {
+            tb = nt - rg.seg_j0 * rg.seg_C;
+            ta = nt - (rg.seg_j0 + seg_count) * rg.seg_C > 0 ? nt - (rg.seg_j0 + seg_count) * rg.seg_C : 0;
+        }
+        if (tb > ta) {
+            const size_t total = (size_t)(tb - ta) * 6 * V;
+            const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+            k_adjoint_coef<<<blocks, 256, 0, st>>>(x, c, lat.ev_fac, V, ta, tb, lat.coef);
+            ephmc::count_launch(1);
+            EPHMC_CUDA(cudaGetLastError());
+        }
+        rg.coef = lat.coef;
+    }
     kern<<<grid, T, smem, st>>>(x, c, lat.ev_src, lat.ev_fac, lat.nbr, qstack, Minv, V, nt, R, pref, force, rg);
     ephmc::count_launch(1);
     EPHMC_CUDA(cudaGetLastError());

@@ -1046,7 +1046,8 @@ int ephmc_ctx_destroy(ephmc_ctx *c) {
     cudaSetDevice(c->device);
     void *bufs[] = {c->x,         c->force,        c->M,          c->G,        c->A,
                     c->B,         c->qstack,       c->jobs,       c->lat.ev_src, c->lat.ev_fac,
-                    c->lat.nbr,   c->lat.rev,      c->scratch,    c->work,     c->cc_part};
+                    c->lat.nbr,   c->lat.rev,      c->lat.coef,   c->scratch,  c->work,
+                    c->cc_part};
     for (void *b : bufs)
         if (b) cudaFree(b);
     fa_forget_tables(c->scratch);
@@ -1127,6 +1128,8 @@ static int ctx_create_impl(ephmc_ctx **out, unsigned l1, unsigned l2, const unsi
     ALLOC(c->lat.ev_fac, sizeof(int) * 6 * V);
     ALLOC(c->lat.nbr, sizeof(int) * 3 * V);
     ALLOC(c->lat.rev, sizeof(int) * 3 * V);
+    ALLOC(c->lat.coef, sizeof(float) * 6 * V * nt);
+    c->lat.coef_nt = (int)nt;
     ALLOC(c->work, sizeof(double) * VV * 4);
     ALLOC(c->cc_part, sizeof(double) * (size_t)nt * V * 9);
     ALLOC(c->x, sizeof(double) * dim);
@@ -1358,6 +1361,7 @@ int ephmc_ctx_memory(const ephmc_ctx *c, size_t *bytes) {
     if (c->G) b += sizeof(double) * VV * c->nt;
     if (c->A) b += 2 * sizeof(double) * VV * c->refine_batch;
     b += sizeof(double) * VV + sizeof(int) * ((size_t)c->V + lu_sync_words((int)c->V));  // LU panel store, pivots
+    b += sizeof(float) * 6 * (size_t)c->V * c->nt;                                      // force sweep coefficients
     b += c->seg_bytes + (c->blas_ws ? kBlasWorkspace : 0);  // segmented mixed force
     b += stab_bytes(c->stab);                               // stabilised chain
     *bytes = b;

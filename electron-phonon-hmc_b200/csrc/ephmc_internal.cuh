@@ -63,6 +63,11 @@ struct LatticeDev {
     // own block, as on lattices of one row): the FP32 force sweep then keeps
     // only their offset (adjoint.cu)
     bool nb_in_events = false;
+    // the packed FP32 force sweep's stencil coefficients, [nt][6][V] floats:
+    // coef[t][e][j] = (float)(t_k - kappa_k x[t][f]), f = ev_fac[e][j],
+    // k = f % 3, filled by the sweep's launcher for the slices it covers
+    float *coef = nullptr;
+    int coef_nt = 0;
 };
 
 // Host helper: build the event tables; returns EPHMC_OK or EPHMC_ERR_LATTICE.
@@ -156,6 +161,9 @@ struct AdjointRange {
     int seg_C = 0, seg_j0 = 0;
     bool seg_regions = false;
     const double *y_start = nullptr;
+    // set by the FP32 sweep's launcher: the slices' coefficient table
+    // (LatticeDev::coef) of its packed instances
+    const float *coef = nullptr;
 };
 
 struct SliceJob {
