@@ -126,8 +126,35 @@ __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoin
         }
     }
 
+    // The packed sweep does not use fac: with R <= 3 it holds the next slice's
+    // q rows, copied from the stack (cp.async) while the slice is computed.
+    Real *qn = fac;
+    const bool qpre = kPack && R <= 3;
+    const bool q16 = (reinterpret_cast<uintptr_t>(qstack) & 15) == 0 && (V & 3) == 0;
+    auto prefetch_q = [&](int s, Real *dst) {
+        if (s == q_id_slice || (rg.q_top != nullptr && s == rg.t1 - 1)) return;  // e_c or the checkpoint
+        const QT *qs = qstack + (size_t)(s - rg.t0) * VV + (size_t)c0 * V;
+        const int n = nvec * V;
+        if (q16) {
+            for (int f = 4 * tid; f < n; f += 4 * T)
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                 (unsigned)__cvta_generic_to_shared(dst + f)),
+                             "l"(qs + f)
+                             : "memory");
+        } else {
+            for (int f = tid; f < n; f += T)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst + f)),
+                             "l"(qs + f)
+                             : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (qpre && rg.t0 < rg.t1) prefetch_q(rg.t0, q);
+
     for (int t = rg.t0; t < rg.t1; ++t) {
-        __syncthreads();
+        if (qpre) asm volatile("cp.async.wait_group 0;" ::: "memory");  // this thread's copies of q(t)
+        __syncthreads();  // everyone's; every thread is past slice t - 1 (qn is free)
+        if (qpre && t + 1 < rg.t1) prefetch_q(t + 1, qn);
         // the sites' stencil coefficients: the packed sweep loads them from the
         // slice's coefficient table (coalesced, before the barrier below); the
         // others form the slice's link coefficients in fac and gather them
@@ -157,7 +184,7 @@ __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoin
             // the segment's last q is its checkpoint, kept in FP64
             const double *qs = rg.q_top + (size_t)c0 * V;
             for (int f = tid; f < nvec * V; f += T) q[f] = (Real)(QT)qs[f];
-        } else {
+        } else if (!qpre) {
             const QT *qs = qstack + (size_t)(t - rg.t0) * VV + (size_t)c0 * V;
             for (int f = tid; f < nvec * V; f += T) q[f] = (Real)qs[f];
         }
@@ -259,6 +286,11 @@ __global__ void __launch_bounds__(WIDE ? (S == 4 ? 640 : 320) : 512, 1) k_adjoin
         Real *tmp = y;
         y = yn;
         yn = tmp;
+        if (qpre) {
+            tmp = q;
+            q = qn;
+            qn = tmp;
+        }
     }
     if (MODE != 2 && rg.y_out != nullptr) {
         Real *yo = static_cast<Real *>(rg.y_out) + (size_t)c0 * V;
