@@ -121,14 +121,17 @@ def test_lu_against_numpy(gpu):
             assert np.array_equal(ipiv - 1, piv)
 
 
-@pytest.mark.parametrize("shape", [(6, 1, 8), (5, 1, 12), (1, 6, 8)])
+@pytest.mark.parametrize("shape", [(6, 1, 8), (5, 1, 12), (1, 6, 8), (41, 41, 12)])
 def test_chain_lattice_forces_agree(gpu, restated, shape):
     """Lattices of one row (L2 = 1) make every site its own upper neighbour:
     the incoming copy of that link sorts inside the site's own event block,
     so the FP32 shared-memory force sweep keeps its neighbour table there
-    instead of the packed offsets (one column, L1 = 1, still packs).  The
-    FP64 adjoint and the mixed force against the reference algorithm on the
-    GPU (itself pinned to the reference's fixtures above)."""
+    instead of the packed offsets (one column, L1 = 1, still packs).  41x41
+    (V = 1681, odd), Nt = 12 (mixed-force segments of 3 slices) runs the
+    packed sweep with three vectors per CTA, so it prefetches the next
+    slice's stack rows, 4 bytes per copy (V is not a multiple of 4).  The FP64 adjoint and the mixed force against the
+    reference algorithm on the GPU (itself pinned to the reference's
+    fixtures above)."""
     import ephmc
     from oracle import Model
     l1, l2, nt = shape
